@@ -1,0 +1,243 @@
+"""ctypes/numpy front end of the CPU oracle.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline leg as the checker, never by the product.
+
+Two oracles live under this directory:
+  * libeh_oracle.so (eh_oracle.c): a C restatement of the reference hot path;
+  * _ref/eh_ref (ref_driver.cpp): the reference storage engine itself,
+    compiled from its own sources, driven by hand-written generated-shape
+    query code.
+Both are built by oracle/Makefile.
+"""
+import ctypes
+import json
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libeh_oracle.so")
+REF_BIN = os.path.join(HERE, "_ref", "eh_ref")
+
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
+_lib = None
+
+
+def build(ref=True):
+    """Compile the restatement (and, when the reference tree is present, the
+    reference engine driver)."""
+    subprocess.check_call(["make", "-s", "-C", HERE, "restate"])
+    if ref and os.path.isdir(os.environ.get("EH_REFERENCE", "/root/reference")):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref",
+                               "REF=" + os.environ.get("EH_REFERENCE", "/root/reference")])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build(ref=False)
+        L = ctypes.CDLL(LIB_PATH)
+        L.eho_rand64.restype = ctypes.c_uint64
+        L.eho_rand64.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+        L.eho_gen_er.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, _u32p, _u32p]
+        L.eho_rmat_thresholds.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, _u32p]
+        L.eho_gen_rmat.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, _u32p, _u32p, _u32p]
+        L.eho_chunglu_cdf.argtypes = [ctypes.c_uint32, ctypes.c_double, _u64p]
+        L.eho_gen_chunglu.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, _u64p, _u32p, _u32p]
+        L.eho_preprocess.restype = ctypes.c_uint64
+        L.eho_preprocess.argtypes = [_u32p, _u32p, ctypes.c_uint64, ctypes.c_int, _u32p, _u32p,
+                                     ctypes.POINTER(ctypes.c_uint32)]
+        L.eho_trie_build.restype = ctypes.c_uint64
+        L.eho_trie_build.argtypes = [_u32p, _u32p, ctypes.c_uint64, _u32p, _u64p, _u32p,
+                                     ctypes.POINTER(ctypes.c_uint32)]
+        L.eho_is_sparse.restype = ctypes.c_int
+        L.eho_is_sparse.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+        L.eho_hybrid_type.restype = ctypes.c_int
+        L.eho_hybrid_type.argtypes = [_u32p, ctypes.c_uint64]
+        L.eho_range_bitset_bytes.restype = ctypes.c_uint64
+        L.eho_range_bitset_bytes.argtypes = [_u32p, ctypes.c_uint64]
+        L.eho_range_bitset_build.restype = ctypes.c_uint64
+        L.eho_range_bitset_build.argtypes = [_u32p, ctypes.c_uint64, _u8p]
+        L.eho_intersect.restype = ctypes.c_uint64
+        L.eho_intersect.argtypes = [_u32p, ctypes.c_uint64, _u32p, ctypes.c_uint64, ctypes.c_void_p]
+        for q in ("eho_triangle", "eho_clique4", "eho_lollipop", "eho_barbell"):
+            f = getattr(L, q)
+            f.restype = ctypes.c_uint64
+            f.argtypes = [_u32p, ctypes.c_uint32, _u64p, _u32p]
+        L.eho_triangle_per_vertex.argtypes = [_u32p, ctypes.c_uint32, _u64p, _u32p, _u64p]
+        L.eho_triangle_annot.argtypes = [_u32p, ctypes.c_uint32, _u64p, _u32p, _u64p]
+        L.eho_mlp_loss_grad.restype = ctypes.c_double
+        L.eho_mlp_loss_grad.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int), _f64p, _f64p, _f64p,
+                                        ctypes.c_int, ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+# ------------------------------------------------------------- generators
+def rmat_thresholds(a=0.57, b=0.19, c=0.19):
+    t = np.zeros(3, np.uint32)
+    lib().eho_rmat_thresholds(a, b, c, t)
+    return t
+
+
+def gen_er(seed, n, m):
+    u = np.empty(m, np.uint32)
+    v = np.empty(m, np.uint32)
+    lib().eho_gen_er(seed, n, m, u, v)
+    return u, v
+
+
+def gen_rmat(seed, scale, m, a=0.57, b=0.19, c=0.19):
+    u = np.empty(m, np.uint32)
+    v = np.empty(m, np.uint32)
+    lib().eho_gen_rmat(seed, scale, m, rmat_thresholds(a, b, c), u, v)
+    return u, v
+
+
+def chunglu_cdf(n, gamma):
+    cdf = np.empty(n, np.uint64)
+    lib().eho_chunglu_cdf(n, gamma, cdf)
+    return cdf
+
+
+def gen_chunglu(seed, n, m, gamma):
+    u = np.empty(m, np.uint32)
+    v = np.empty(m, np.uint32)
+    lib().eho_gen_chunglu(seed, n, m, chunglu_cdf(n, gamma), u, v)
+    return u, v
+
+
+def preprocess(u, v, symmetric=False):
+    u = np.ascontiguousarray(u, np.uint32)
+    v = np.ascontiguousarray(v, np.uint32)
+    m = len(u)
+    cap = max(1, 2 * m if symmetric else m)
+    s = np.empty(cap, np.uint32)
+    d = np.empty(cap, np.uint32)
+    nodes = ctypes.c_uint32(0)
+    r = lib().eho_preprocess(u, v, m, 1 if symmetric else 0, s, d, ctypes.byref(nodes))
+    return s[:r].copy(), d[:r].copy(), nodes.value
+
+
+# ------------------------------------------------------------------- trie
+class Trie:
+    """Two-level trie as sorted head + CSR of child sets."""
+
+    def __init__(self, c0, c1):
+        c0 = np.ascontiguousarray(c0, np.uint32)
+        c1 = np.ascontiguousarray(c1, np.uint32)
+        n = len(c0)
+        head = np.empty(max(1, n), np.uint32)
+        off = np.empty(max(1, n) + 1, np.uint64)
+        vals = np.empty(max(1, n), np.uint32)
+        nh = ctypes.c_uint32(0)
+        r = lib().eho_trie_build(c0, c1, n, head, off, vals, ctypes.byref(nh))
+        self.head = head[: nh.value].copy()
+        self.off = off[: nh.value + 1].copy()
+        self.vals = vals[:r].copy()
+
+    @property
+    def n_head(self):
+        return len(self.head)
+
+    def child(self, i):
+        return self.vals[self.off[i]: self.off[i + 1]]
+
+    def layouts(self):
+        """hybrid layout code per child set (0 = RANGE_BITSET, 1 = UINTEGER)."""
+        L = lib()
+        return np.array([L.eho_hybrid_type(np.ascontiguousarray(self.child(i)), len(self.child(i)))
+                         for i in range(self.n_head)], np.uint8)
+
+    def _args(self):
+        return (self.head, self.n_head, self.off, self.vals)
+
+    def triangle(self):
+        return int(lib().eho_triangle(*self._args()))
+
+    def clique4(self):
+        return int(lib().eho_clique4(*self._args()))
+
+    def lollipop(self):
+        return int(lib().eho_lollipop(*self._args()))
+
+    def barbell(self):
+        return int(lib().eho_barbell(*self._args()))
+
+    def triangle_per_vertex(self):
+        per = np.empty(max(1, self.n_head), np.uint64)
+        lib().eho_triangle_per_vertex(*self._args(), per)
+        return per[: self.n_head]
+
+
+def hybrid_type(a):
+    a = np.ascontiguousarray(a, np.uint32)
+    return int(lib().eho_hybrid_type(a, len(a)))
+
+
+def range_bitset(a):
+    a = np.ascontiguousarray(a, np.uint32)
+    nb = int(lib().eho_range_bitset_bytes(a, len(a)))
+    out = np.zeros(max(nb, 1), np.uint8)
+    lib().eho_range_bitset_build(a, len(a), out)
+    return out[:nb]
+
+
+def intersect(a, b):
+    a = np.ascontiguousarray(a, np.uint32)
+    b = np.ascontiguousarray(b, np.uint32)
+    out = np.empty(max(1, min(len(a), len(b))), np.uint32)
+    c = lib().eho_intersect(a, len(a), b, len(b), out.ctypes.data)
+    return out[:c].copy()
+
+
+def mlp_loss_grad(dims, params, x, y):
+    dims_c = (ctypes.c_int * len(dims))(*dims)
+    params = np.ascontiguousarray(params, np.float64)
+    grad = np.zeros_like(params)
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.ascontiguousarray(y, np.float64)
+    loss = lib().eho_mlp_loss_grad(len(dims) - 1, dims_c, params, x, y, x.shape[0], grad.ctypes.data)
+    return loss, grad
+
+
+# ------------------------------------------------------- reference engine
+def write_edge_file(path, src, dst):
+    src = np.ascontiguousarray(src, np.uint32)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    with open(path, "wb") as f:
+        f.write(b"EHEDGE01")
+        f.write(np.uint64(len(src)).tobytes())
+        f.write(src.tobytes())
+        f.write(dst.tobytes())
+
+
+def ref_available():
+    return os.path.exists(REF_BIN)
+
+
+def ref_query(mode, edges_path, repeats=1, threads=None, timeout=None):
+    """Run the reference engine on an edge file; returns its JSON dict."""
+    env = dict(os.environ)
+    if threads:
+        env["EH_REF_THREADS"] = str(threads)
+    with tempfile.TemporaryDirectory() as td:
+        env["TMPDIR"] = td
+        out = subprocess.run([REF_BIN, mode, edges_path, str(repeats)], env=env, capture_output=True,
+                             text=True, timeout=timeout, check=True).stdout
+    return json.loads(out.strip().splitlines()[-1])
+
+
+def ref_query_edges(mode, src, dst, repeats=1, threads=None, timeout=None):
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "edges.bin")
+        write_edge_file(p, src, dst)
+        return ref_query(mode, p, repeats, threads, timeout)

@@ -1,0 +1,483 @@
+/* Reference-engine driver for the CPU oracle and the timed CPU baseline.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is compiled (by oracle/Makefile)
+ * against the reference storage engine's own sources, which stay where they
+ * lie; nothing here ships in the product.
+ *
+ * The Scala query compiler cannot run in this image (no JVM), so the
+ * per-query C++ it would emit is written out here by hand, statement by
+ * statement in the shape EHGenerator.scala emits for the plans pinned by
+ * QueryPlannerTest.scala:
+ *   - emitHeadParForeach  query_compiler/.../codegen/query/EHGenerator.scala:273-300
+ *   - emitBuildCode       EHGenerator.scala:302-354
+ *   - emitForeach         EHGenerator.scala:384-397
+ *   - annotation code     EHGenerator.scala:399-480
+ *   - bag wrapper         EHGenerator.scala:728-838
+ * Plans: triangle / 4-clique one bag, order [a,b,(c),(d)]
+ * (QueryPlannerTest.scala:78-96); lollipop / barbell two bags with an
+ * annotated bag (QueryPlannerTest.scala:199-230, IROptimizerTest.scala:189).
+ *
+ * Modes (all print one JSON line on stdout):
+ *   eh_ref triangle|clique4|lollipop|barbell <edges> [repeats]
+ *   eh_ref trie_dump <edges> <out.bin>      dump the reference trie
+ *   eh_ref setops <pairs.bin> <out.bin>     per-pair ops::set_intersect
+ * <edges> is a .tsv (two uint32 columns) or an edge file written by the
+ * project's graph generator ("EHEDGE01" header, u64 n, u32 src[n], u32 dst[n]).
+ *
+ * Values are dictionary-encoded before the trie build the way the
+ * reference's loader does it: one order-preserving code per distinct value
+ * over both columns (storage_engine/src/Encoding.cpp:21-48 assigns keys in
+ * sorted value order).  The encoding here is a sort-unique + lower_bound
+ * with the same result.
+ */
+#include <sys/stat.h>
+#include <sys/time.h>
+#include <sched.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "Trie.hpp"
+#include "TrieBuilder.hpp"
+#include "TrieIterator.hpp"
+#include "trie/TrieBlock.hpp"
+#include "utils/thread_pool.hpp"
+#include "utils/timer.hpp"
+
+typedef ParMemoryBuffer MB;
+
+std::size_t eh_ref_num_threads() {
+  const char* e = getenv("EH_REF_THREADS");
+  if (e && atoi(e) > 0) return (std::size_t)atoi(e);
+  cpu_set_t set;
+  CPU_ZERO(&set);
+  if (sched_getaffinity(0, sizeof(set), &set) == 0) {
+    int c = CPU_COUNT(&set);
+    if (c > 0) return (std::size_t)std::min(c, 500);
+  }
+  long n = sysconf(_SC_NPROCESSORS_ONLN);
+  return n > 0 ? (std::size_t)std::min(n, 500L) : 1;
+}
+
+static double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+/* ---------------------------------------------------------------- input */
+static bool read_edges(const std::string& path, std::vector<uint32_t>& s, std::vector<uint32_t>& d) {
+  FILE* f = fopen(path.c_str(), "rb");
+  if (!f) return false;
+  char magic[8] = {0};
+  if (fread(magic, 1, 8, f) == 8 && memcmp(magic, "EHEDGE01", 8) == 0) {
+    uint64_t n = 0;
+    if (fread(&n, 8, 1, f) != 1) { fclose(f); return false; }
+    s.resize(n); d.resize(n);
+    if (n && (fread(s.data(), 4, n, f) != n || fread(d.data(), 4, n, f) != n)) { fclose(f); return false; }
+    fclose(f);
+    return true;
+  }
+  fseek(f, 0, SEEK_SET);
+  unsigned long a, b;
+  while (fscanf(f, "%lu %lu", &a, &b) == 2) { s.push_back((uint32_t)a); d.push_back((uint32_t)b); }
+  fclose(f);
+  return true;
+}
+
+/* order-preserving dictionary encoding over both columns */
+static uint32_t encode(std::vector<uint32_t>& s, std::vector<uint32_t>& d) {
+  std::vector<uint32_t> vals(s);
+  vals.insert(vals.end(), d.begin(), d.end());
+  std::sort(vals.begin(), vals.end());
+  vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+  bool identity = vals.empty() || (vals.front() == 0 && vals.back() + 1 == vals.size());
+  if (!identity) {
+    for (auto* col : {&s, &d})
+      for (auto& x : *col) x = (uint32_t)(std::lower_bound(vals.begin(), vals.end(), x) - vals.begin());
+  }
+  return (uint32_t)vals.size();
+}
+
+static Trie<void*, MB>* build_edge_trie(const std::string& dir, std::vector<uint32_t>& s,
+                                        std::vector<uint32_t>& d, uint32_t ndistinct) {
+  mkdir(dir.c_str(), 0755);
+  mkdir((dir + "/ram").c_str(), 0755);
+  std::vector<std::vector<uint32_t>> cols(2);
+  cols[0] = s;
+  cols[1] = d;
+  std::vector<uint32_t> max_set_size(2, ndistinct);
+  std::vector<void*> annotation;  // Edge is not annotated
+  return new Trie<void*, MB>(dir, &max_set_size, &cols, &annotation);
+}
+
+/* ------------------------------------------------- generated-shape bags */
+
+/* TriangleAgg(;z) :- Edge(a,b),Edge(b,c),Edge(a,c),z:long<-[COUNT(*)]. */
+static long bag_triangle(Trie<void*, MB>* Trie_Edge_0_1, const std::string& out) {
+  Trie<long, MB>* Trie_TriangleAgg_ = new Trie<long, MB>(out, 0, true);
+  long result;
+  {
+    ParTrieBuilder<long, MB> Builders(Trie_TriangleAgg_, 3);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_b(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_b_c(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_c(Trie_Edge_0_1);
+    const size_t count_a = Builders.build_aggregated_set(Iterators_Edge_a_b.head, Iterators_Edge_a_c.head);
+    (void)count_a;
+    par::reducer<long> annotation_a(0, [&](long a, long b) { return a + b; });
+    Builders.par_foreach_aggregate([&](const size_t tid, const uint32_t a_d) {
+      TrieBuilder<long, MB>* Builder = Builders.builders.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_b = Iterators_Edge_a_b.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_b_c = Iterators_Edge_b_c.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_c = Iterators_Edge_a_c.iterators.at(tid);
+      Iterator_Edge_a_b->get_next_block(0, a_d);
+      Iterator_Edge_a_c->get_next_block(0, a_d);
+      const size_t count_b =
+          Builder->build_aggregated_set(Iterator_Edge_a_b->get_block(1), Iterator_Edge_b_c->get_block(0));
+      (void)count_b;
+      long annotation_b = (long)0;
+      Builder->foreach_aggregate([&](const uint32_t b_d) {
+        Iterator_Edge_b_c->get_next_block(0, b_d);
+        const size_t count_c =
+            Builder->build_aggregated_set(Iterator_Edge_b_c->get_block(1), Iterator_Edge_a_c->get_block(1));
+        const long intermediate_c = (long)1 * (count_c * 1);
+        annotation_b += intermediate_c;
+      });
+      annotation_a.update(tid, annotation_b);
+    });
+    Builders.trie->annotation = annotation_a.evaluate(0);
+    result = Builders.trie->annotation;
+  }
+  delete Trie_TriangleAgg_;
+  return result;
+}
+
+/* FliqueAgg(;z) :- Edge(a,b),Edge(b,c),Edge(a,c),Edge(a,d),Edge(b,d),Edge(c,d),z:long<-[COUNT(*)]. */
+static long bag_clique4(Trie<void*, MB>* Trie_Edge_0_1, const std::string& out) {
+  typedef const TrieBlock<hybrid, MB>* TB;
+  Trie<long, MB>* Trie_FliqueAgg_ = new Trie<long, MB>(out, 0, true);
+  long result;
+  {
+    ParTrieBuilder<long, MB> Builders(Trie_FliqueAgg_, 4);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_b(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_b_c(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_c(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_d(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_b_d(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_c_d(Trie_Edge_0_1);
+    std::vector<TB> a_sets;
+    a_sets.push_back(Iterators_Edge_a_b.head);
+    a_sets.push_back(Iterators_Edge_a_c.head);
+    a_sets.push_back(Iterators_Edge_a_d.head);
+    const size_t count_a = Builders.build_aggregated_set(&a_sets);
+    (void)count_a;
+    par::reducer<long> annotation_a(0, [&](long a, long b) { return a + b; });
+    Builders.par_foreach_aggregate([&](const size_t tid, const uint32_t a_d) {
+      TrieBuilder<long, MB>* Builder = Builders.builders.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_b = Iterators_Edge_a_b.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_b_c = Iterators_Edge_b_c.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_c = Iterators_Edge_a_c.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_d = Iterators_Edge_a_d.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_b_d = Iterators_Edge_b_d.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_c_d = Iterators_Edge_c_d.iterators.at(tid);
+      Iterator_Edge_a_b->get_next_block(0, a_d);
+      Iterator_Edge_a_c->get_next_block(0, a_d);
+      Iterator_Edge_a_d->get_next_block(0, a_d);
+      std::vector<TB> b_sets;
+      b_sets.push_back(Iterator_Edge_a_b->get_block(1));
+      b_sets.push_back(Iterator_Edge_b_c->get_block(0));
+      b_sets.push_back(Iterator_Edge_b_d->get_block(0));
+      const size_t count_b = Builder->build_aggregated_set(&b_sets);
+      (void)count_b;
+      long annotation_b = (long)0;
+      Builder->foreach_aggregate([&](const uint32_t b_d) {
+        Iterator_Edge_b_c->get_next_block(0, b_d);
+        Iterator_Edge_b_d->get_next_block(0, b_d);
+        std::vector<TB> c_sets;
+        c_sets.push_back(Iterator_Edge_b_c->get_block(1));
+        c_sets.push_back(Iterator_Edge_a_c->get_block(1));
+        c_sets.push_back(Iterator_Edge_c_d->get_block(0));
+        const size_t count_c = Builder->build_aggregated_set(&c_sets);
+        (void)count_c;
+        long annotation_c = (long)0;
+        Builder->foreach_aggregate([&](const uint32_t c_d) {
+          Iterator_Edge_c_d->get_next_block(0, c_d);
+          std::vector<TB> d_sets;
+          d_sets.push_back(Iterator_Edge_a_d->get_block(1));
+          d_sets.push_back(Iterator_Edge_b_d->get_block(1));
+          d_sets.push_back(Iterator_Edge_c_d->get_block(1));
+          const size_t count_d = Builder->build_aggregated_set(&d_sets);
+          const long intermediate_d = (long)1 * (count_d * 1);
+          annotation_c += intermediate_d;
+        });
+        annotation_b += annotation_c;
+      });
+      annotation_a.update(tid, annotation_b);
+    });
+    Builders.trie->annotation = annotation_a.evaluate(0);
+    result = Builders.trie->annotation;
+  }
+  delete Trie_FliqueAgg_;
+  return result;
+}
+
+/* bag_1_a_b_c(a;z) :- Edge(a,c),Edge(b,c),Edge(a,b),z:long<-[SUM over (b,c) of 1].
+ * Materialised 1-level annotated trie (QueryPlannerTest.scala:199-212). */
+static Trie<long, MB>* bag_triangle_annot(Trie<void*, MB>* Trie_Edge_0_1, const std::string& out) {
+  mkdir(out.c_str(), 0755);
+  mkdir((out + "/ram").c_str(), 0755);
+  Trie<long, MB>* Trie_bag_1_a_b_c_0 = new Trie<long, MB>(out, 1, true);
+  {
+    ParTrieBuilder<long, MB> Builders(Trie_bag_1_a_b_c_0, 3);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_c(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_b_c(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_b(Trie_Edge_0_1);
+    const size_t count_a = Builders.build_set(Iterators_Edge_a_c.head, Iterators_Edge_a_b.head);
+    Builders.allocate_annotation();
+    Builders.par_foreach_builder([&](const size_t tid, const uint32_t a_i, const uint32_t a_d) {
+      TrieBuilder<long, MB>* Builder = Builders.builders.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_c = Iterators_Edge_a_c.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_b_c = Iterators_Edge_b_c.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_b = Iterators_Edge_a_b.iterators.at(tid);
+      Iterator_Edge_a_c->get_next_block(0, a_d);
+      Iterator_Edge_a_b->get_next_block(0, a_d);
+      const size_t count_b =
+          Builder->build_aggregated_set(Iterator_Edge_b_c->get_block(0), Iterator_Edge_a_b->get_block(1));
+      (void)count_b;
+      long annotation_b = (long)0;
+      Builder->foreach_aggregate([&](const uint32_t b_d) {
+        Iterator_Edge_b_c->get_next_block(0, b_d);
+        const size_t count_c =
+            Builder->build_aggregated_set(Iterator_Edge_a_c->get_block(1), Iterator_Edge_b_c->get_block(1));
+        const long intermediate_c = (long)1 * (count_c * 1);
+        annotation_b += intermediate_c;
+      });
+      Builder->set_annotation(annotation_b, a_i, a_d);
+    });
+    Builders.trie->num_rows = count_a;
+  }
+  return Trie_bag_1_a_b_c_0;
+}
+
+/* LollipopAgg(;z) :- Edge(a,d) ⋈ bag_1(a;z)  (root bag, order [a,d]) */
+static long bag_lollipop_root(Trie<void*, MB>* Trie_Edge_0_1, Trie<long, MB>* Trie_bag_1, const std::string& out) {
+  Trie<long, MB>* Trie_LollipopAgg_ = new Trie<long, MB>(out, 0, true);
+  long result;
+  {
+    ParTrieBuilder<long, MB> Builders(Trie_LollipopAgg_, 2);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_d(Trie_Edge_0_1);
+    ParTrieIterator<long, MB> Iterators_bag_1_a(Trie_bag_1);
+    const size_t count_a = Builders.build_aggregated_set(Iterators_Edge_a_d.head, Iterators_bag_1_a.head);
+    (void)count_a;
+    par::reducer<long> annotation_a(0, [&](long a, long b) { return a + b; });
+    Builders.par_foreach_aggregate([&](const size_t tid, const uint32_t a_d) {
+      TrieBuilder<long, MB>* Builder = Builders.builders.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_d = Iterators_Edge_a_d.iterators.at(tid);
+      TrieIterator<long, MB>* Iterator_bag_1_a = Iterators_bag_1_a.iterators.at(tid);
+      Iterator_Edge_a_d->get_next_block(0, a_d);
+      const size_t count_d = Builder->build_aggregated_set(Iterator_Edge_a_d->get_block(1));
+      const long intermediate_d = (long)1 * (count_d * 1);
+      const long intermediate_a = (long)1 * Iterator_bag_1_a->get_annotation(0, a_d) * intermediate_d;
+      annotation_a.update(tid, intermediate_a);
+    });
+    Builders.trie->annotation = annotation_a.evaluate(0);
+    result = Builders.trie->annotation;
+  }
+  delete Trie_LollipopAgg_;
+  return result;
+}
+
+/* BarbellAgg(;w) :- Edge(a,x) ⋈ bag_1(a;z) ⋈ bag_1(x;z)  (root bag, order [a,x];
+ * the two triangle bags are deduplicated into one, IROptimizer.scala:64) */
+static long bag_barbell_root(Trie<void*, MB>* Trie_Edge_0_1, Trie<long, MB>* Trie_bag_1, const std::string& out) {
+  Trie<long, MB>* Trie_BarbellAgg_ = new Trie<long, MB>(out, 0, true);
+  long result;
+  {
+    ParTrieBuilder<long, MB> Builders(Trie_BarbellAgg_, 2);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_x(Trie_Edge_0_1);
+    ParTrieIterator<long, MB> Iterators_bag_1_a(Trie_bag_1);
+    ParTrieIterator<long, MB> Iterators_bag_1_x(Trie_bag_1);
+    const size_t count_a = Builders.build_aggregated_set(Iterators_Edge_a_x.head, Iterators_bag_1_a.head);
+    (void)count_a;
+    par::reducer<long> annotation_a(0, [&](long a, long b) { return a + b; });
+    Builders.par_foreach_aggregate([&](const size_t tid, const uint32_t a_d) {
+      TrieBuilder<long, MB>* Builder = Builders.builders.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_x = Iterators_Edge_a_x.iterators.at(tid);
+      TrieIterator<long, MB>* Iterator_bag_1_a = Iterators_bag_1_a.iterators.at(tid);
+      TrieIterator<long, MB>* Iterator_bag_1_x = Iterators_bag_1_x.iterators.at(tid);
+      Iterator_Edge_a_x->get_next_block(0, a_d);
+      const size_t count_x =
+          Builder->build_aggregated_set(Iterator_Edge_a_x->get_block(1), Iterator_bag_1_x->get_block(0));
+      (void)count_x;
+      long annotation_x = (long)0;
+      Builder->foreach_aggregate([&](const uint32_t x_d) {
+        const long intermediate_x = (long)1 * Iterator_bag_1_x->get_annotation(0, x_d);
+        annotation_x += intermediate_x;
+      });
+      const long intermediate_a = (long)1 * Iterator_bag_1_a->get_annotation(0, a_d) * annotation_x;
+      annotation_a.update(tid, intermediate_a);
+    });
+    Builders.trie->annotation = annotation_a.evaluate(0);
+    result = Builders.trie->annotation;
+  }
+  delete Trie_BarbellAgg_;
+  return result;
+}
+
+/* ------------------------------------------------------------ dumps */
+static void put(FILE* f, const void* p, size_t n) { fwrite(p, 1, n, f); }
+
+/* Writes, for the head and for each child set: type, cardinality, range,
+ * number_of_bytes and the layout bytes.  Layout bytes are the reference's
+ * own: uinteger = sorted u32; range_bitset = [u64 start word][u64 words][u32
+ * per-word rank] (layouts/range_bitset.hpp:123-157). */
+static int trie_dump(Trie<void*, MB>* t, const char* outp) {
+  FILE* f = fopen(outp, "wb");
+  if (!f) return 1;
+  TrieBlock<hybrid, MB>* head = t->getHead();
+  const Set<hybrid>* hs = head->get_set();
+  auto dump_set = [&](const Set<hybrid>* s) {
+    uint8_t ty = (uint8_t)s->type;
+    uint32_t card = s->cardinality, range = s->range;
+    uint64_t nb = s->number_of_bytes;
+    put(f, &ty, 1); put(f, &card, 4); put(f, &range, 4); put(f, &nb, 8);
+    put(f, s->get_data(), nb);
+  };
+  dump_set(hs);
+  hs->foreach_index([&](uint32_t a_i, uint32_t a_d) {
+    TrieBlock<hybrid, MB>* nb = head->get_next_block(a_i, a_d, t->memoryBuffers);
+    uint32_t v = a_d;
+    uint8_t present = nb != NULL;
+    put(f, &v, 4); put(f, &present, 1);
+    if (nb) dump_set(nb->get_set());
+  });
+  fclose(f);
+  return 0;
+}
+
+/* pairs file: u64 npairs, then per pair u32 na, u32 A[na], u32 nb, u32 B[nb].
+ * out file, per pair: u8 typeA, u8 typeB, u64 bytesA, bytesA of layout A,
+ * u64 count (aggregate mode), u8 result type, u32 n, u32 elems[n]
+ * (materialize mode, elements via Set::foreach). */
+static int setops(const char* inp, const char* outp) {
+  FILE* f = fopen(inp, "rb");
+  if (!f) return 1;
+  uint64_t np = 0;
+  if (fread(&np, 8, 1, f) != 1) { fclose(f); return 1; }
+  FILE* o = fopen(outp, "wb");
+  if (!o) { fclose(f); return 1; }
+  std::vector<uint32_t> A, B;
+  for (uint64_t p = 0; p < np; p++) {
+    uint32_t na, nb;
+    if (fread(&na, 4, 1, f) != 1) return 1;
+    A.resize(na);
+    if (na && fread(A.data(), 4, na, f) != na) return 1;
+    if (fread(&nb, 4, 1, f) != 1) return 1;
+    B.resize(nb);
+    if (nb && fread(B.data(), 4, nb, f) != nb) return 1;
+    const uint32_t ra = na ? A.back() - A.front() : 0, rb = nb ? B.back() - B.front() : 0;
+    const size_t ba = hybrid::get_number_of_bytes(na, ra) + 64, bb = hybrid::get_number_of_bytes(nb, rb) + 64;
+    std::vector<uint8_t> bufA(sizeof(Set<hybrid>) + ba, 0), bufB(sizeof(Set<hybrid>) + bb, 0);
+    Set<hybrid>* sA = new (bufA.data()) Set<hybrid>();
+    Set<hybrid>* sB = new (bufB.data()) Set<hybrid>();
+    sA->from_array(sA->get_data(), A.data(), na);
+    sB->from_array(sB->get_data(), B.data(), nb);
+    /* result buffer sized the way TrieBuilder does it (TrieBuilder.cpp:15-24),
+       with slack for the bitset result that starts at max(start words) */
+    const size_t rbytes = std::max(ba, bb) * 2 + 256;
+    std::vector<uint8_t> bufC(sizeof(Set<hybrid>) + rbytes, 0);
+    Set<hybrid>* sC = new (bufC.data()) Set<hybrid>();
+    const Set<hybrid>* cA = sA;
+    const Set<hybrid>* cB = sB;
+    const uint64_t cnt = ops::set_intersect(cA, cB);
+    sC = ops::set_intersect(sC, cA, cB);
+    std::vector<uint32_t> out;
+    sC->foreach([&](uint32_t x) { out.push_back(x); });
+    uint8_t ta = sA->type, tb = sB->type, tc = sC->type;
+    uint64_t nba = sA->number_of_bytes;
+    uint32_t nout = (uint32_t)out.size();
+    put(o, &ta, 1); put(o, &tb, 1); put(o, &nba, 8); put(o, sA->get_data(), nba);
+    put(o, &cnt, 8); put(o, &tc, 1); put(o, &nout, 4);
+    if (nout) put(o, out.data(), 4 * (size_t)nout);
+  }
+  fclose(f);
+  fclose(o);
+  printf("{\"mode\": \"setops\", \"pairs\": %llu}\n", (unsigned long long)np);
+  return 0;
+}
+
+static std::string scratch_dir() {
+  const char* t = getenv("TMPDIR");
+  std::string base = t ? t : "/tmp";
+  char buf[64];
+  snprintf(buf, sizeof buf, "/eh_ref_%d", (int)getpid());
+  std::string d = base + buf;
+  mkdir(d.c_str(), 0755);
+  return d;
+}
+
+int main(int argc, char** argv) {
+  if (argc < 3) {
+    fprintf(stderr, "usage: eh_ref triangle|clique4|lollipop|barbell <edges> [repeats]\n"
+                    "       eh_ref trie_dump <edges> <out>\n       eh_ref setops <pairs> <out>\n");
+    return 2;
+  }
+  const std::string mode = argv[1];
+  if (mode == "setops") return argc > 3 ? setops(argv[2], argv[3]) : 2;
+
+  std::vector<uint32_t> s, d;
+  if (!read_edges(argv[2], s, d) || s.empty()) {
+    fprintf(stderr, "cannot read edges from %s\n", argv[2]);
+    return 1;
+  }
+  const uint32_t nd = encode(s, d);
+  const std::string dir = scratch_dir();
+  thread_pool::initializeThreadPool();
+  const double tb0 = now_s();
+  Trie<void*, MB>* Trie_Edge_0_1 = build_edge_trie(dir + "/Edge_0_1", s, d, nd);
+  const double build_s = now_s() - tb0;
+
+  if (mode == "trie_dump") {
+    int rc = argc > 3 ? trie_dump(Trie_Edge_0_1, argv[3]) : 2;
+    printf("{\"mode\": \"trie_dump\", \"rows\": %zu, \"build_s\": %.6f}\n", s.size(), build_s);
+    thread_pool::deleteThreadPool();
+    return rc;
+  }
+
+  const int repeats = argc > 3 ? std::max(1, atoi(argv[3])) : 1;
+  std::vector<double> times;
+  long count = 0;
+  for (int r = 0; r < repeats; r++) {
+    auto query_timer = timer::start_clock();
+    if (mode == "triangle") {
+      count = bag_triangle(Trie_Edge_0_1, dir + "/TriangleAgg");
+    } else if (mode == "clique4") {
+      count = bag_clique4(Trie_Edge_0_1, dir + "/FliqueAgg");
+    } else if (mode == "lollipop" || mode == "barbell") {
+      Trie<long, MB>* bag1 = bag_triangle_annot(Trie_Edge_0_1, dir + "/bag_1_a_b_c");
+      count = mode == "lollipop" ? bag_lollipop_root(Trie_Edge_0_1, bag1, dir + "/LollipopAgg")
+                                 : bag_barbell_root(Trie_Edge_0_1, bag1, dir + "/BarbellAgg");
+      delete bag1;
+    } else {
+      fprintf(stderr, "unknown mode %s\n", mode.c_str());
+      return 2;
+    }
+    times.push_back(timer::stop_clock(query_timer));
+  }
+  thread_pool::deleteThreadPool();
+  std::vector<double> sorted(times);
+  std::sort(sorted.begin(), sorted.end());
+  printf("{\"mode\": \"%s\", \"count\": %ld, \"count_u64\": %llu, \"rows\": %zu, \"distinct\": %u, "
+         "\"threads\": %zu, \"build_s\": %.6f, \"query_s_median\": %.9f, \"query_s\": [",
+         mode.c_str(), count, (unsigned long long)(uint64_t)count, s.size(), nd, NUM_THREADS, build_s,
+         sorted[sorted.size() / 2]);
+  for (size_t i = 0; i < times.size(); i++) printf("%s%.9f", i ? ", " : "", times[i]);
+  printf("]}\n");
+  fflush(stdout);
+  _exit(0); /* the reference's pool threads are parked; skip their teardown */
+}
