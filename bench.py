@@ -1,0 +1,356 @@
+"""Benchmark: R-MAT scale-22 triangle COUNT on B200 (learned vs heuristic
+layouts), with the reference CPU engine as the baseline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step = one triangle COUNT query over the resident trie):
+R-MAT scale 22, edge factor 16 (67,108,864 samples), a/b/c/d =
+0.57/0.19/0.19/0.05, seed 42; symmetrised, self-loops dropped, deduped,
+relabelled by degree, src < dst (64,152,167 rows).  The trie is built on
+the device before timing (the reference's QUERY TIME excludes the load,
+README.md:137).  The timed step is the generic-join bag: plan + intersection
+kernel + count to host.  Every step's count is checked against the
+reference engine's 2,110,948,863.
+
+One JSON line on rank 0.  N > 1: every rank holds the trie, runs a
+round-robin share of the work items, and the partial counts meet in one
+8-byte NCCL all-reduce; time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SCALE, EF, SEED = 22, 16, 42
+ABCD = (0.57, 0.19, 0.19)
+WORKLOAD = "R-MAT scale 22, edge factor 16, a/b/c/d 0.57/0.19/0.19/0.05, seed 42, degree-ordered src<dst; " \
+           "triangle COUNT (TriangleAgg)"
+METRIC = "R-MAT-22 triangle-count ms: learned vs heuristic layout on B200; CPU ref"
+
+
+def golden():
+    with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+        return json.load(f)["synthetic"]["rmat_s22_ef16_s42"]
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits", "-lms", "100"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# --------------------------------------------------------------- CPU side
+def run_reference(rows_src, rows_dst, repeats, threads=None, timeout=1800):
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    return O.ref_query_edges("triangle", rows_src, rows_dst, repeats=repeats, threads=threads, timeout=timeout)
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_arm(args):
+    """The reference's own CPU engine (compiled from its sources) on the same
+    workload, on all host cores.  Inputs come from the CPU oracle's generator
+    (identical edge list, checked by sha1 in the tests)."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    g = golden()
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/eh_ref was not built (no reference tree)"}))
+        return 0
+    u, v = O.gen_rmat(SEED, SCALE, EF << SCALE, *ABCD)
+    s, d, _ = O.preprocess(u, v)
+    del u, v
+    r = run_reference(s, d, args.warmup + args.steps)
+    times = r["query_s"][args.warmup:]
+    assert r["count_u64"] == g["triangle"], r
+    ms = [1e3 * x for x in times]
+    value = statistics.median(ms)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "ms", "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sum(ms) / len(ms), "higher_is_better": False,
+            "scaling": "strong", "vs_baseline": None, "dtype": "uint32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "engine": "reference storage engine compiled from its sources "
+                                                      "(oracle/_ref/eh_ref), generated-shape TriangleAgg bag",
+                       "threads": r["threads"], "timer": "reference timer::stop_clock over the bag"},
+            "count": r["count_u64"],
+            "cpu_baseline": {"value": value, "unit": "ms", "cores": r["threads"], "kind": "reference",
+                             "sample": "full workload, %d timed runs after %d warm-up" % (args.steps, args.warmup)},
+            "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# --------------------------------------------------------------- GPU side
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the intersection kernel from the committed
+    ncu summary (profiles/triangle_kernel_rmat22.json), if present."""
+    p = os.path.join(ROOT, "profiles", "triangle_kernel_rmat22.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    return None
+
+
+def train_layout_model(E, trie, steps_per_layout=1):
+    """Profile-guided cost model: time every staged set under each layout
+    (engine-logged per-item device cycles), train the MLP on the logs with
+    the engine's own kernels, and return it with its fit statistics."""
+    from emptyheaded_b200 import learn
+    return learn.train_from_trie(E, trie, passes=steps_per_layout)
+
+
+def ours_arm(args):
+    import numpy as np
+    import torch
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    import emptyheaded_b200 as E
+
+    ctx = E.Context(local if world > 1 else 0)
+    E._default = ctx
+    g = golden()
+    # ---- input pipeline and trie build (untimed, like the reference's load)
+    t0 = time.time()
+    u, v = E.gen_rmat(SEED, SCALE, EF << SCALE, *ABCD, ctx=ctx)
+    s, d, nodes = E.preprocess(u, v, ctx=ctx)
+    u.free()
+    v.free()
+    trie = E.Trie(s, d, ctx=ctx)
+    info_h = trie.info()
+    build_s = time.time() - t0
+
+    shard = (rank, world)
+
+    def step(tr):
+        c, st = tr.count("triangle", stats=True, shard=shard)
+        if world > 1:
+            tc = torch.tensor([c], dtype=torch.int64, device="cuda")
+            torch.distributed.all_reduce(tc)
+            c = int(tc.item()) & ((1 << 64) - 1)
+        return c, st
+
+    # L2 flush buffer (larger than the 126 MB L2)
+    flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")
+
+    def timed(tr, steps, warmup):
+        for _ in range(warmup):
+            c, _ = step(tr)
+            assert c == g["triangle"], c
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        qms, kms, launches = [], [], 0
+        wall0 = time.time()
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            c, st = step(tr)
+            assert c == g["triangle"], c
+            qms.append(st["query_ms"])
+            kms.append(st["kernel_ms"])
+            launches += st["launches"]
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        wall = time.time() - wall0
+        return qms, kms, launches, st, wall
+
+    # ---- heuristic layouts
+    qh, kh, lh, st_h, wall_h = timed(trie, args.steps, args.warmup)
+    # ---- learned layouts (model trained on this engine's logged timings)
+    learn_info = {}
+    try:
+        model, learn_info = train_layout_model(E, trie)
+        trie.relayout(policy=E.LEARNED, model=model)
+        info_l = trie.info()
+        ql, kl, ll, st_l, wall_l = timed(trie, args.steps, args.warmup)
+        learn_info["layout_hist"] = {"uint": info_l["n_uinteger"], "bitset": info_l["n_range_bitset"],
+                                     "block": info_l["n_block_bitset"]}
+    except Exception as ex:  # the learned arm must not hide the measurement
+        learn_info = {"error": repr(ex)[:300]}
+        ql, kl, ll, st_l, wall_l = qh, kh, lh, st_h, wall_h
+
+    # max over ranks
+    def rmax(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    ms_h = rmax(statistics.mean(qh))
+    ms_l = rmax(statistics.mean(ql))
+    kern_l = rmax(statistics.mean(kl))
+    kern_h = rmax(statistics.mean(kh))
+
+    # ---- e2e through the host-buffer entry: CSR in pinned host memory,
+    # copied to the device every step (plus the trie index build), count back
+    e2e = None
+    if world == 1:
+        head, off, vals, _ = trie.export()
+        head_p = torch.from_numpy(head).pin_memory().numpy()
+        off_p = torch.from_numpy(off.view(np.int64)).pin_memory().numpy().view(np.uint64)
+        vals_p = torch.from_numpy(vals.view(np.int32)).pin_memory().numpy().view(np.uint32)
+        h2d = head_p.nbytes + off_p.nbytes + vals_p.nbytes
+        pol = E.LEARNED if "error" not in learn_info else E.HEURISTIC
+        mdl = model if "error" not in learn_info else None
+        for _ in range(max(1, args.warmup // 2)):
+            c = E.count_host_csr(head_p, off_p, vals_p, nodes, policy=pol, model=mdl, ctx=ctx)
+            assert c == g["triangle"]
+        ev = []
+        for _ in range(max(3, args.steps // 2)):
+            torch.cuda.synchronize()
+            a = time.perf_counter()
+            c = E.count_host_csr(head_p, off_p, vals_p, nodes, policy=pol, model=mdl, ctx=ctx)
+            ev.append(1e3 * (time.perf_counter() - a))
+            assert c == g["triangle"]
+        e2e = {"value": statistics.median(ev), "unit": "ms", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8,
+               "path": "eh_query_count_host_csr: pinned host CSR -> device, trie index + layouts, count, result to host"}
+
+    # ---- CPU baseline (rank 0, N = 1): the reference engine on the same rows
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        hs, hd = s.numpy(), d.numpy()
+        try:
+            r = run_reference(hs, hd, 3)
+            if r:
+                cpu = {"value": 1e3 * statistics.median(r["query_s"]), "unit": "ms", "cores": r["threads"],
+                       "kind": "reference",
+                       "sample": "full R-MAT-22 triangle COUNT, median of 3 runs, trie build excluded "
+                                 "(reference build %.1f s, sort serialised)" % r["build_s"],
+                       "count": r["count_u64"]}
+                assert r["count_u64"] == g["triangle"]
+        except Exception as ex:
+            cpu = {"value": None, "unit": "ms", "cores": cpu_threads(), "kind": "reference", "sample": repr(ex)[:200]}
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        alg = st_l["algorithmic_bytes"]
+        achieved = alg / (kern_l * 1e-3) / 1e9
+        traffic = profile_traffic()
+        line = {
+            "metric": METRIC, "value": ms_l, "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_l, "higher_is_better": False, "scaling": "strong",
+            "vs_baseline": None, "dtype": "uint32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "rows": info_h["rows"], "nodes": nodes, "layout": "learned",
+                       "heuristic_ms": ms_h, "learned_ms": ms_l, "learned_speedup": ms_h / ms_l,
+                       "heuristic_kernel_ms": kern_h, "learned_kernel_ms": kern_l,
+                       "l2": "trie (%.2f GB) larger than L2, and a 256 MB buffer written between steps"
+                             % (info_h["device_bytes"] / 1e9),
+                       "trie_build_s": build_s, "parallelism": "shards of work items" if world > 1 else "single GPU",
+                       "learned": learn_info},
+            "count": g["triangle"],
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_kind": peak_kind + " (hbm_gbs)",
+                         "algorithmic_bytes": alg, "kernel": "eh::triangle_kernel<false>"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(ll / max(1, args.steps)) * args.steps,
+        }
+        line["clocks"] = args.sampler.stop()
+        print(json.dumps(line), flush=True)
+    trie.free()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return reference_arm(args)
+    _, _, local = dist_env()
+    args.sampler = ClockSampler(local)
+    args.sampler.start()
+    return ours_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

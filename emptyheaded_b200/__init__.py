@@ -1,0 +1,470 @@
+"""B200-native storage-engine hot path of EmptyHeaded: trie construction,
+hybrid uint / bitset / block-bitset set layouts, set intersection and the
+generic-join COUNT plans, as sm_100a CUDA kernels behind a C ABI
+(include/eh_b200.h).
+
+This module is a thin ctypes front end over that ABI, named after the
+reference's storage-engine API:
+
+    Trie            Trie<A,M> built from an encoded binary relation
+                    (storage_engine/src/Trie.cpp:380-510)
+    Trie.count()    a generated COUNT bag (EHGenerator.scala:728-838) run on
+                    the device
+    set_intersect   ops::set_intersect (trie/set/ops/intersection/set.hpp)
+
+It never computes on the host: if the shared library or a GPU is missing,
+calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libeh_b200.so")
+
+# status codes and enums (include/eh_b200.h)
+EH_OK = 0
+STATUS_NAMES = {1: "INVALID", 2: "CUDA", 3: "OOM", 4: "TIMEOUT", 5: "UNSUPPORTED", 6: "IO", 7: "NO_DEVICE"}
+RANGE_BITSET, UINTEGER, BLOCK_BITSET = 0, 1, 3
+HEURISTIC, LEARNED, FORCED = 0, 1, 2
+QUERIES = {"triangle": 0, "clique4": 1, "lollipop": 2, "barbell": 3}
+
+
+class EHError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s (%s)" % (msg, STATUS_NAMES.get(status, status)))
+        self.status = status
+
+
+class LayoutConfig(ctypes.Structure):
+    _fields_ = [("policy", ctypes.c_int), ("forced_layout", ctypes.c_int), ("model", ctypes.c_void_p),
+                ("max_bitset_bytes", ctypes.c_uint64)]
+
+
+class TrieInfo(ctypes.Structure):
+    _fields_ = [("rows", ctypes.c_uint64), ("n_head", ctypes.c_uint32), ("n_nodes", ctypes.c_uint32),
+                ("head_layout", ctypes.c_uint32), ("n_uinteger", ctypes.c_uint32),
+                ("n_range_bitset", ctypes.c_uint32), ("n_block_bitset", ctypes.c_uint32),
+                ("bitset_words", ctypes.c_uint64), ("block_count", ctypes.c_uint64),
+                ("device_bytes", ctypes.c_uint64), ("max_set", ctypes.c_uint32), ("build_ms", ctypes.c_float)]
+
+
+class ExecConfig(ctypes.Structure):
+    _fields_ = [("warps_per_block", ctypes.c_int), ("chunk_pairs", ctypes.c_int), ("big_item_pairs", ctypes.c_int),
+                ("smem_words", ctypes.c_int), ("record_timings", ctypes.c_int), ("spin_limit", ctypes.c_uint64),
+                ("shard_index", ctypes.c_int), ("shard_count", ctypes.c_int)]
+
+
+class QueryStats(ctypes.Structure):
+    _fields_ = [("query_ms", ctypes.c_float), ("kernel_ms", ctypes.c_float), ("launches", ctypes.c_uint32),
+                ("work_items", ctypes.c_uint64), ("wedges", ctypes.c_uint64),
+                ("algorithmic_bytes", ctypes.c_uint64), ("timed_out", ctypes.c_int)]
+
+
+_lib = None
+
+_P = ctypes.c_void_p
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+
+
+def lib():
+    """The loaded shared library (raises when it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise EHError(5, "libeh_b200.so is not built; run python -m emptyheaded_b200.build")
+        L = ctypes.CDLL(LIB_PATH)
+        L.eh_last_error.restype = ctypes.c_char_p
+        L.eh_version.restype = ctypes.c_char_p
+        sig = {
+            "eh_context_create": [ctypes.c_int, ctypes.POINTER(_P)],
+            "eh_context_destroy": [_P],
+            "eh_context_sync": [_P],
+            "eh_context_stream": [_P, ctypes.POINTER(_P)],
+            "eh_device_alloc": [_P, ctypes.c_uint64, ctypes.POINTER(_P)],
+            "eh_device_free": [_P, _P],
+            "eh_memcpy": [_P, _P, _P, ctypes.c_uint64],
+            "eh_graph_er": [_P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(_P),
+                            ctypes.POINTER(_P)],
+            "eh_graph_rmat": [_P, ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
+                              ctypes.c_double, ctypes.POINTER(_P), ctypes.POINTER(_P)],
+            "eh_graph_chunglu": [_P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double,
+                                 ctypes.POINTER(_P), ctypes.POINTER(_P)],
+            "eh_graph_preprocess": [_P, _P, _P, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_P),
+                                    ctypes.POINTER(_P), _u64p, _u32p],
+            "eh_trie_build": [_P, _P, _P, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(LayoutConfig),
+                              ctypes.POINTER(_P)],
+            "eh_trie_relayout": [_P, _P, ctypes.POINTER(LayoutConfig)],
+            "eh_trie_free": [_P],
+            "eh_trie_info_get": [_P, ctypes.POINTER(TrieInfo)],
+            "eh_trie_export": [_P, _P, _P, _P, _P],
+            "eh_trie_set_bytes": [_P, ctypes.c_uint32, _P, ctypes.c_uint64, _u64p, ctypes.POINTER(ctypes.c_uint8)],
+            "eh_set_intersect_batch": [_P, _P, _P, ctypes.c_uint32, _P, _P, _P, ctypes.c_uint32, _P, _P, _P],
+            "eh_query_count": [_P, _P, ctypes.c_int, ctypes.POINTER(ExecConfig), _u64p, ctypes.POINTER(QueryStats)],
+            "eh_query_count_batched": [_P, _P, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ExecConfig), _P,
+                                       ctypes.POINTER(QueryStats)],
+            "eh_triangle_annotation": [_P, _P, ctypes.POINTER(ExecConfig), _P],
+            "eh_query_count_host_csr": [_P, _P, ctypes.c_uint32, _P, _P, ctypes.c_uint32,
+                                        ctypes.POINTER(LayoutConfig), ctypes.c_int, ctypes.POINTER(ExecConfig), _u64p,
+                                        ctypes.POINTER(QueryStats)],
+            "eh_timing_records": [_P, _P, ctypes.c_uint64, _u64p],
+            "eh_model_create": [_P, ctypes.c_int, _P, ctypes.c_uint64, ctypes.POINTER(_P)],
+            "eh_model_free": [_P],
+            "eh_model_params": [_P, _P, ctypes.c_uint64, _u64p, ctypes.c_int],
+            "eh_model_train": [_P, _P, _P, _P, ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32,
+                               ctypes.POINTER(ctypes.c_float)],
+            "eh_model_loss_grad": [_P, _P, _P, _P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float), _P],
+            "eh_model_predict": [_P, _P, _P, ctypes.c_uint32, _P],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != EH_OK:
+        raise EHError(status, lib().eh_last_error().decode())
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+# ------------------------------------------------------------------ context
+class Context:
+    """Device, stream and events (the role of the reference's thread pool,
+    utils/thread_pool.hpp:16-41)."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        _check(lib().eh_context_create(device, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().eh_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        _check(lib().eh_context_sync(self.h))
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        _check(lib().eh_context_stream(self.h, ctypes.byref(s)))
+        return s.value
+
+
+_default = None
+
+
+def default_context():
+    global _default
+    if _default is None:
+        _default = Context(0)
+    return _default
+
+
+class DeviceArray:
+    """A uint32 device array owned by the engine (eh_device_alloc)."""
+
+    def __init__(self, ctx, ptr, n):
+        self.ctx, self.ptr, self.n = ctx, ptr, n
+
+    def free(self):
+        if self.ptr:
+            _check(lib().eh_device_free(self.ctx.h, ctypes.c_void_p(self.ptr)))
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def numpy(self):
+        out = np.empty(self.n, np.uint32)
+        if self.n:
+            _check(lib().eh_memcpy(self.ctx.h, _ptr(out), ctypes.c_void_p(self.ptr), 4 * self.n))
+        return out
+
+
+def _pair(ctx, fn, m, *args):
+    u, v = ctypes.c_void_p(), ctypes.c_void_p()
+    _check(fn(ctx.h, *args, ctypes.byref(u), ctypes.byref(v)))
+    return DeviceArray(ctx, u.value, m), DeviceArray(ctx, v.value, m)
+
+
+def gen_er(seed, n, m, ctx=None):
+    ctx = ctx or default_context()
+    return _pair(ctx, lib().eh_graph_er, m, seed, n, m)
+
+
+def gen_rmat(seed, scale, m, a=0.57, b=0.19, c=0.19, ctx=None):
+    ctx = ctx or default_context()
+    return _pair(ctx, lib().eh_graph_rmat, m, seed, scale, m, a, b, c)
+
+
+def gen_chunglu(seed, n, m, gamma, ctx=None):
+    ctx = ctx or default_context()
+    return _pair(ctx, lib().eh_graph_chunglu, m, seed, n, m, gamma)
+
+
+def preprocess(u, v, symmetric=False, ctx=None):
+    """Device edge samples -> (src, dst, nodes): the encoded Edge relation."""
+    ctx = ctx or default_context()
+    s, d = ctypes.c_void_p(), ctypes.c_void_p()
+    rows, nodes = ctypes.c_uint64(), ctypes.c_uint32()
+    _check(lib().eh_graph_preprocess(ctx.h, ctypes.c_void_p(u.ptr), ctypes.c_void_p(v.ptr), u.n,
+                                     1 if symmetric else 0, ctypes.byref(s), ctypes.byref(d), ctypes.byref(rows),
+                                     ctypes.byref(nodes)))
+    return DeviceArray(ctx, s.value, rows.value), DeviceArray(ctx, d.value, rows.value), nodes.value
+
+
+def _layout_cfg(policy=HEURISTIC, forced=UINTEGER, model=None, max_bitset_bytes=0):
+    c = LayoutConfig()
+    c.policy = policy
+    c.forced_layout = forced
+    c.model = model.h.value if model is not None else None
+    c.max_bitset_bytes = max_bitset_bytes
+    return c
+
+
+def _exec_cfg(warps=0, chunk=0, smem_words=0, record=False, shard=(0, 1)):
+    e = ExecConfig()
+    e.warps_per_block = warps
+    e.chunk_pairs = chunk
+    e.big_item_pairs = 0
+    e.smem_words = smem_words
+    e.record_timings = 1 if record else 0
+    e.spin_limit = 0
+    e.shard_index, e.shard_count = shard
+    return e
+
+
+# --------------------------------------------------------------------- trie
+class Trie:
+    """Two-level trie over an encoded binary relation, resident on the GPU.
+
+    Mirrors Trie<A,M>(path, max_set_sizes, attr_in, annotations)
+    (storage_engine/src/Trie.cpp:380-510): rows in any order, duplicates
+    allowed; the head is the distinct first-column values, each with the
+    sorted set of its second-column values in a hybrid layout.
+    """
+
+    def __init__(self, col0, col1, policy=HEURISTIC, forced=UINTEGER, model=None, ctx=None, max_bitset_bytes=0):
+        self.ctx = ctx or default_context()
+        cfg = _layout_cfg(policy, forced, model, max_bitset_bytes)
+        h = ctypes.c_void_p()
+        if isinstance(col0, DeviceArray):
+            _check(lib().eh_trie_build(self.ctx.h, ctypes.c_void_p(col0.ptr), ctypes.c_void_p(col1.ptr), col0.n, 1,
+                                       ctypes.byref(cfg), ctypes.byref(h)))
+        else:
+            c0 = np.ascontiguousarray(col0, np.uint32)
+            c1 = np.ascontiguousarray(col1, np.uint32)
+            if c0.shape != c1.shape:
+                raise ValueError("columns differ in length")
+            _check(lib().eh_trie_build(self.ctx.h, _ptr(c0), _ptr(c1), len(c0), 0, ctypes.byref(cfg),
+                                       ctypes.byref(h)))
+        self.h = h
+
+    def free(self):
+        if getattr(self, "h", None):
+            lib().eh_trie_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def info(self):
+        i = TrieInfo()
+        _check(lib().eh_trie_info_get(self.h, ctypes.byref(i)))
+        return {k: getattr(i, k) for k, _ in TrieInfo._fields_}
+
+    def relayout(self, policy=HEURISTIC, forced=UINTEGER, model=None, max_bitset_bytes=0):
+        cfg = _layout_cfg(policy, forced, model, max_bitset_bytes)
+        _check(lib().eh_trie_relayout(self.ctx.h, self.h, ctypes.byref(cfg)))
+
+    def export(self):
+        """(head, off, vals, layout) host copies (what Trie::foreach walks)."""
+        inf = self.info()
+        nh, rows = inf["n_head"], inf["rows"]
+        head = np.empty(max(nh, 1), np.uint32)
+        off = np.empty(nh + 1, np.uint64)
+        vals = np.empty(max(rows, 1), np.uint32)
+        lay = np.empty(max(nh, 1), np.uint8)
+        _check(lib().eh_trie_export(self.h, _ptr(head), _ptr(off), _ptr(vals), _ptr(lay)))
+        return head[:nh], off, vals[:rows], lay[:nh]
+
+    def set_bytes(self, i):
+        """Reference-format bytes of child set i (None: the head set) and its layout."""
+        idx = 0xFFFFFFFF if i is None else i
+        n = ctypes.c_uint64()
+        lay = ctypes.c_uint8()
+        _check(lib().eh_trie_set_bytes(self.h, idx, None, 0, ctypes.byref(n), ctypes.byref(lay)))
+        out = np.empty(max(n.value, 1), np.uint8)
+        _check(lib().eh_trie_set_bytes(self.h, idx, _ptr(out), n.value, ctypes.byref(n), ctypes.byref(lay)))
+        return out[: n.value], lay.value
+
+    def count(self, query="triangle", warps=0, chunk=0, smem_words=0, record=False, stats=False, shard=(0, 1)):
+        """Run a named COUNT plan; returns the count (and stats if asked).
+        shard=(i, n) runs the i-th of n round-robin shares of the work items
+        (the partial counts of the n shares sum to the count)."""
+        e = _exec_cfg(warps, chunk, smem_words, record, shard)
+        r = ctypes.c_uint64()
+        st = QueryStats()
+        _check(lib().eh_query_count(self.ctx.h, self.h, QUERIES[query], ctypes.byref(e), ctypes.byref(r),
+                                    ctypes.byref(st)))
+        if stats:
+            return r.value, {k: getattr(st, k) for k, _ in QueryStats._fields_}
+        return r.value
+
+    def triangle_annotation(self):
+        nh = self.info()["n_head"]
+        out = np.zeros(max(nh, 1), np.uint64)
+        e = _exec_cfg()
+        _check(lib().eh_triangle_annotation(self.ctx.h, self.h, ctypes.byref(e), _ptr(out)))
+        return out[:nh]
+
+
+def count_batched(tries, query="triangle", chunk=0, stats=False):
+    ctx = tries[0].ctx
+    arr = (ctypes.c_void_p * len(tries))(*[t.h.value for t in tries])
+    res = np.zeros(len(tries), np.uint64)
+    e = _exec_cfg(chunk=chunk)
+    st = QueryStats()
+    _check(lib().eh_query_count_batched(ctx.h, arr, len(tries), QUERIES[query], ctypes.byref(e), _ptr(res),
+                                        ctypes.byref(st)))
+    if stats:
+        return res, {k: getattr(st, k) for k, _ in QueryStats._fields_}
+    return res
+
+
+def count_host_csr(head, off, vals, n_nodes, query="triangle", policy=HEURISTIC, model=None, ctx=None, stats=False):
+    """Host CSR in, count out: the reference-facing call with host buffers."""
+    ctx = ctx or default_context()
+    cfg = _layout_cfg(policy, UINTEGER, model)
+    e = _exec_cfg()
+    r = ctypes.c_uint64()
+    st = QueryStats()
+    _check(lib().eh_query_count_host_csr(ctx.h, _ptr(head), len(head), _ptr(off), _ptr(vals), n_nodes,
+                                         ctypes.byref(cfg), QUERIES[query], ctypes.byref(e), ctypes.byref(r),
+                                         ctypes.byref(st)))
+    if stats:
+        return r.value, {k: getattr(st, k) for k, _ in QueryStats._fields_}
+    return r.value
+
+
+def timing_records(ctx=None):
+    ctx = ctx or default_context()
+    n = ctypes.c_uint64()
+    _check(lib().eh_timing_records(ctx.h, None, 0, ctypes.byref(n)))
+    out = np.empty((max(n.value, 1), 8), np.float32)
+    _check(lib().eh_timing_records(ctx.h, _ptr(out), n.value, ctypes.byref(n)))
+    return out[: n.value]
+
+
+# ------------------------------------------------------------------ set ops
+def set_intersect(sets, layouts, pairs, materialize=False, ctx=None):
+    """Pairwise ops::set_intersect on the device.
+
+    sets: list of sorted uint32 arrays; layouts: per-set layout codes;
+    pairs: (k, 2) array of set indices.  Returns counts (and the
+    materialized intersections as a list when asked)."""
+    ctx = ctx or default_context()
+    sizes = np.array([len(s) for s in sets], np.uint64)
+    off = np.zeros(len(sets) + 1, np.uint64)
+    np.cumsum(sizes, out=off[1:])
+    elems = np.ascontiguousarray(np.concatenate([np.asarray(s, np.uint32) for s in sets])
+                                 if len(sets) else np.zeros(0, np.uint32), np.uint32)
+    if elems.size == 0:
+        elems = np.zeros(1, np.uint32)
+    lay = np.ascontiguousarray(layouts, np.uint8)
+    pairs = np.ascontiguousarray(pairs, np.uint32).reshape(-1, 2)
+    pa = np.ascontiguousarray(pairs[:, 0])
+    pb = np.ascontiguousarray(pairs[:, 1])
+    counts = np.zeros(max(len(pa), 1), np.uint64)
+    out_off = out = None
+    if materialize:
+        room = np.minimum(sizes[pa], sizes[pb])
+        out_off = np.zeros(len(pa), np.uint64)
+        if len(pa) > 1:
+            np.cumsum(room[:-1], out=out_off[1:])
+        out = np.zeros(max(int(room.sum()), 1), np.uint32)
+    _check(lib().eh_set_intersect_batch(ctx.h, _ptr(elems), _ptr(off), len(sets), _ptr(lay), _ptr(pa), _ptr(pb),
+                                        len(pa), _ptr(counts), _ptr(out_off), _ptr(out)))
+    counts = counts[: len(pa)]
+    if materialize:
+        return counts, [out[int(o): int(o) + int(c)].copy() for o, c in zip(out_off, counts)]
+    return counts
+
+
+# -------------------------------------------------------------------- model
+class Model:
+    """Small fp32 MLP trained and evaluated by the engine's own kernels."""
+
+    def __init__(self, dims, seed=0, ctx=None):
+        self.ctx = ctx or default_context()
+        self.dims = list(dims)
+        d = (ctypes.c_int * len(dims))(*dims)
+        h = ctypes.c_void_p()
+        _check(lib().eh_model_create(self.ctx.h, len(dims) - 1, d, seed, ctypes.byref(h)))
+        self.h = h
+
+    def free(self):
+        if getattr(self, "h", None):
+            lib().eh_model_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def params(self):
+        n = ctypes.c_uint64()
+        _check(lib().eh_model_params(self.h, None, 0, ctypes.byref(n), 0))
+        out = np.empty(n.value, np.float32)
+        _check(lib().eh_model_params(self.h, _ptr(out), n.value, ctypes.byref(n), 0))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        n = ctypes.c_uint64()
+        _check(lib().eh_model_params(self.h, _ptr(p), len(p), ctypes.byref(n), 1))
+
+    def train(self, x, y, lr=1e-2, steps=1):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        loss = ctypes.c_float()
+        _check(lib().eh_model_train(self.ctx.h, self.h, _ptr(x), _ptr(y), x.shape[0], lr, steps, ctypes.byref(loss)))
+        return loss.value
+
+    def loss_grad(self, x, y):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        loss = ctypes.c_float()
+        g = np.empty(len(self.params()), np.float32)
+        _check(lib().eh_model_loss_grad(self.ctx.h, self.h, _ptr(x), _ptr(y), x.shape[0], ctypes.byref(loss),
+                                        _ptr(g)))
+        return loss.value, g
+
+    def predict(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.empty((x.shape[0], self.dims[-1]), np.float32)
+        _check(lib().eh_model_predict(self.ctx.h, self.h, _ptr(x), x.shape[0], _ptr(y)))
+        return y

@@ -1,0 +1,161 @@
+// Shared definitions for the B200 storage-engine kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+
+#include "eh_b200.h"
+
+namespace eh {
+
+constexpr int kWarp = 32;
+constexpr uint32_t kFull = 0xffffffffu;
+
+// ---------------------------------------------------------------- errors
+// Every entry point returns an eh_status; the message of the last failure
+// on the calling thread is kept for eh_last_error().
+void set_error(const std::string& msg);
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+#define EH_CUDA(call)                                                                  \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      throw ::eh::Error{EH_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+
+#define EH_CHECK_LAUNCH() EH_CUDA(cudaGetLastError())
+
+#define EH_REQUIRE(cond, code, msg)                           \
+  do {                                                        \
+    if (!(cond)) throw ::eh::Error{(code), std::string(msg)}; \
+  } while (0)
+
+inline int ceil_div(uint64_t a, uint64_t b) { return (int)((a + b - 1) / b); }
+
+inline int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+// ------------------------------------------------------- device buffers
+// Stream-ordered device allocations (cudaMallocAsync) owned by RAII
+// handles; a trie and its layouts live in a handful of these.
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaStream_t s = 0;
+  DevBuf() = default;
+  DevBuf(size_t count, cudaStream_t stream) { alloc(count, stream); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p; n = o.n; s = o.s;
+      o.p = nullptr; o.n = 0;
+    }
+    return *this;
+  }
+  void alloc(size_t count, cudaStream_t stream) {
+    release();
+    s = stream;
+    n = count;
+    if (count) {
+      cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T), stream);
+      if (e != cudaSuccess) {
+        p = nullptr;
+        n = 0;
+        cudaGetLastError();
+        throw Error{EH_ERR_OOM, "device allocation of " + std::to_string(count * sizeof(T)) + " bytes failed"};
+      }
+    }
+  }
+  void release() {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+    n = 0;
+  }
+  ~DevBuf() { release(); }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// --------------------------------------------------------- device helpers
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// inclusive warp scan
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T v) {
+  const uint32_t l = lane_id();
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T t = __shfl_up_sync(kFull, v, o);
+    if (l >= (uint32_t)o) v += t;
+  }
+  return v;
+}
+
+// ------------------------------------------------------------------- rng
+// splitmix64 as a counter-based generator: draw i of a stream is a pure
+// function of (seed, i); the host oracle uses the same function.
+__host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+// draw `index` of the stream whose seed was mixed once: splitmix64(seed)
+__host__ __device__ __forceinline__ uint64_t rand64(uint64_t seed_mixed, uint64_t index) {
+  return splitmix64(seed_mixed ^ splitmix64(index));
+}
+
+inline int bits_for(uint64_t maxv) {
+  int b = 1;
+  while (b < 64 && (maxv >> b)) b++;
+  return b;
+}
+
+// ------------------------------------------------------------ primitives
+// Device-wide exclusive scan of n elements (in may equal out).  Returns
+// the total through *total_dev when non-null (device pointer, one T).
+template <typename T>
+void exclusive_scan(const T* in, T* out, uint64_t n, T* total_dev, cudaStream_t s);
+
+// LSD radix sort of n 64-bit keys on their low `bits` bits, in place
+// (tmp must hold n keys).
+void radix_sort_u64(uint64_t* keys, uint64_t* tmp, uint64_t n, int bits, cudaStream_t s);
+
+// Keep the first of each run of equal keys (keys sorted).  Writes the
+// compacted keys to out and the count to *count_host (synchronises).
+uint64_t unique_sorted_u64(const uint64_t* keys, uint64_t* out, uint64_t n, cudaStream_t s);
+
+// max of n u32 values (synchronises)
+uint32_t max_u32(const uint32_t* a, uint64_t n, cudaStream_t s);
+
+}  // namespace eh

@@ -1,0 +1,252 @@
+// Device-wide primitives written for this engine: exclusive scan, LSD radix
+// sort of 64-bit keys, unique, max.  They replace the reference's TBB sort
+// (storage_engine/src/Trie.cpp:403-404) and its sequential run detection
+// (Trie.cpp:192-224, 291-302) inside the trie build.
+#include "eh_common.cuh"
+
+namespace eh {
+
+// ================================================================== scan
+// Three-phase scan: per-tile reduce, scan of tile sums (recursive), per-tile
+// scan with the tile's offset.  Tile = 256 threads x 8 items.
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+template <typename T>
+__device__ __forceinline__ T block_excl_scan(T v, T* warp_tot, T* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  T inc = warp_incl_scan(v);
+  if (lane == 31) warp_tot[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    T w = lane < (kScanThreads / 32) ? warp_tot[lane] : T(0);
+    T wi = warp_incl_scan(w);
+    if (lane < (kScanThreads / 32)) warp_tot[lane] = wi - w;
+    if (lane == (kScanThreads / 32) - 1) *total = wi;
+  }
+  __syncthreads();
+  return inc - v + warp_tot[wid];
+}
+
+template <typename T>
+__global__ void scan_reduce_kernel(const T* __restrict__ in, uint64_t n, T* __restrict__ tile_sums) {
+  __shared__ T warp_tot[kScanThreads / 32];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    uint64_t i = base + (uint64_t)k * kScanThreads + threadIdx.x;
+    if (i < n) s += in[i];
+  }
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) warp_tot[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    T w = threadIdx.x < (kScanThreads / 32) ? warp_tot[threadIdx.x] : T(0);
+    w = warp_sum(w);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = w;
+  }
+}
+
+template <typename T>
+__global__ void scan_tile_kernel(const T* __restrict__ in, T* __restrict__ out, uint64_t n,
+                                 const T* __restrict__ tile_offsets, T* __restrict__ total_dev) {
+  __shared__ T warp_tot[kScanThreads / 32];
+  __shared__ T tot;
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+  T v[kScanItems];
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    uint64_t i = base + k;
+    v[k] = i < n ? in[i] : T(0);
+    s += v[k];
+  }
+  T ex = block_excl_scan(s, warp_tot, &tot);
+  const T off = tile_offsets ? tile_offsets[blockIdx.x] : T(0);
+  T run = off + ex;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    uint64_t i = base + k;
+    if (i < n) out[i] = run;
+    run += v[k];
+  }
+  if (total_dev && blockIdx.x == gridDim.x - 1 && threadIdx.x == kScanThreads - 1) *total_dev = run;
+}
+
+template <typename T>
+void exclusive_scan(const T* in, T* out, uint64_t n, T* total_dev, cudaStream_t s) {
+  if (n == 0) {
+    if (total_dev) EH_CUDA(cudaMemsetAsync(total_dev, 0, sizeof(T), s));
+    return;
+  }
+  const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+  if (tiles == 1) {
+    scan_tile_kernel<T><<<1, kScanThreads, 0, s>>>(in, out, n, nullptr, total_dev);
+    EH_CHECK_LAUNCH();
+    return;
+  }
+  DevBuf<T> sums(tiles, s);
+  scan_reduce_kernel<T><<<(unsigned)tiles, kScanThreads, 0, s>>>(in, n, sums.p);
+  EH_CHECK_LAUNCH();
+  exclusive_scan<T>(sums.p, sums.p, tiles, nullptr, s);
+  scan_tile_kernel<T><<<(unsigned)tiles, kScanThreads, 0, s>>>(in, out, n, sums.p, total_dev);
+  EH_CHECK_LAUNCH();
+}
+template void exclusive_scan<uint32_t>(const uint32_t*, uint32_t*, uint64_t, uint32_t*, cudaStream_t);
+template void exclusive_scan<uint64_t>(const uint64_t*, uint64_t*, uint64_t, uint64_t*, cudaStream_t);
+
+// ============================================================ radix sort
+// LSD, 8-bit digits.  One pass = histogram per tile (digit-major counters),
+// exclusive scan of the counters, stable scatter.  A tile is 8 warps x 16
+// rounds x 32 keys; each warp ranks its keys stably with __match_any_sync
+// against a warp-private digit histogram in shared memory.
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortRounds = 16;
+constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096 keys
+constexpr int kRadix = 256;
+
+__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint64_t* __restrict__ keys, uint64_t n,
+                                                                  int shift, uint32_t* __restrict__ counts,
+                                                                  uint32_t tiles) {
+  __shared__ uint32_t h[kRadix];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
+#pragma unroll 4
+  for (int r = 0; r < kSortRounds; r++) {
+    uint64_t i = base + (uint64_t)r * kSortThreads + threadIdx.x;
+    if (i < n) atomicAdd(&h[(keys[i] >> shift) & 0xff], 1u);
+  }
+  __syncthreads();
+  counts[(uint64_t)threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint64_t* __restrict__ keys,
+                                                                     uint64_t* __restrict__ out, uint64_t n,
+                                                                     int shift,
+                                                                     const uint32_t* __restrict__ offsets,
+                                                                     uint32_t tiles) {
+  __shared__ uint32_t whist[kSortWarps][kRadix];
+  __shared__ uint32_t tile_off[kRadix];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&whist[0][0])[i] = 0;
+  tile_off[threadIdx.x] = offsets[(uint64_t)threadIdx.x * tiles + blockIdx.x];
+  __syncthreads();
+  // warp w owns keys [base + w*512, base + (w+1)*512), round-major
+  const uint64_t wbase = (uint64_t)blockIdx.x * kSortTile + (uint64_t)wid * (32 * kSortRounds);
+  uint64_t k[kSortRounds];
+  uint32_t pos[kSortRounds];
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int r = 0; r < kSortRounds; r++) {
+    const uint64_t i = wbase + (uint64_t)r * 32 + lane;
+    const bool valid = i < n;
+    k[r] = valid ? keys[i] : 0;
+    const uint32_t d = valid ? (uint32_t)((k[r] >> shift) & 0xff) : 0x100u;
+    const uint32_t peers = __match_any_sync(kFull, d);
+    const uint32_t rank = __popc(peers & lt);
+    const int leader = __ffs(peers) - 1;
+    uint32_t basecnt = 0;
+    if (valid) basecnt = whist[wid][d];
+    __syncwarp();
+    if (valid && lane == leader) whist[wid][d] = basecnt + __popc(peers);
+    __syncwarp();
+    pos[r] = basecnt + rank;  // offset among this warp's keys of digit d
+  }
+  __syncthreads();
+  // per-digit exclusive prefix over warps (thread t owns digit t)
+  {
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; w++) {
+      uint32_t c = whist[w][threadIdx.x];
+      whist[w][threadIdx.x] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kSortRounds; r++) {
+    const uint64_t i = wbase + (uint64_t)r * 32 + lane;
+    if (i < n) {
+      const uint32_t d = (uint32_t)((k[r] >> shift) & 0xff);
+      out[tile_off[d] + whist[wid][d] + pos[r]] = k[r];
+    }
+  }
+}
+
+void radix_sort_u64(uint64_t* keys, uint64_t* tmp, uint64_t n, int bits, cudaStream_t s) {
+  if (n < 2) return;
+  EH_REQUIRE(n < (1ull << 32), EH_ERR_UNSUPPORTED, "radix sort supports fewer than 2^32 keys");
+  const uint32_t tiles = (uint32_t)((n + kSortTile - 1) / kSortTile);
+  DevBuf<uint32_t> counts((uint64_t)kRadix * tiles, s);
+  uint64_t* src = keys;
+  uint64_t* dst = tmp;
+  int passes = 0;
+  for (int shift = 0; shift < bits; shift += 8, passes++) {
+    radix_hist_kernel<<<tiles, kSortThreads, 0, s>>>(src, n, shift, counts.p, tiles);
+    EH_CHECK_LAUNCH();
+    exclusive_scan<uint32_t>(counts.p, counts.p, (uint64_t)kRadix * tiles, nullptr, s);
+    radix_scatter_kernel<<<tiles, kSortThreads, 0, s>>>(src, dst, n, shift, counts.p, tiles);
+    EH_CHECK_LAUNCH();
+    uint64_t* t = src;
+    src = dst;
+    dst = t;
+  }
+  if (src != keys) EH_CUDA(cudaMemcpyAsync(keys, src, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+}
+
+// ================================================================ unique
+__global__ void head_flags_kernel(const uint64_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ flags) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    flags[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+}
+__global__ void compact_kernel(const uint64_t* __restrict__ keys, uint64_t n, const uint32_t* __restrict__ pos,
+                               uint64_t* __restrict__ out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    if (i == 0 || keys[i] != keys[i - 1]) out[pos[i]] = keys[i];
+}
+
+uint64_t unique_sorted_u64(const uint64_t* keys, uint64_t* out, uint64_t n, cudaStream_t s) {
+  if (n == 0) return 0;
+  DevBuf<uint32_t> pos(n, s);
+  DevBuf<uint32_t> total(1, s);
+  const int grid = num_sms() * 8;
+  head_flags_kernel<<<grid, 256, 0, s>>>(keys, n, pos.p);
+  EH_CHECK_LAUNCH();
+  exclusive_scan<uint32_t>(pos.p, pos.p, n, total.p, s);
+  compact_kernel<<<grid, 256, 0, s>>>(keys, n, pos.p, out);
+  EH_CHECK_LAUNCH();
+  uint32_t h = 0;
+  EH_CUDA(cudaMemcpyAsync(&h, total.p, 4, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
+// =================================================================== max
+__global__ void max_kernel(const uint32_t* __restrict__ a, uint64_t n, uint32_t* __restrict__ out) {
+  uint32_t m = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    m = max(m, a[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(kFull, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+uint32_t max_u32(const uint32_t* a, uint64_t n, cudaStream_t s) {
+  DevBuf<uint32_t> out(1, s);
+  EH_CUDA(cudaMemsetAsync(out.p, 0, 4, s));
+  if (n) {
+    max_kernel<<<num_sms() * 4, 256, 0, s>>>(a, n, out.p);
+    EH_CHECK_LAUNCH();
+  }
+  uint32_t h = 0;
+  EH_CUDA(cudaMemcpyAsync(&h, out.p, 4, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
+}  // namespace eh

@@ -1,0 +1,686 @@
+// Generic-join COUNT executors for the named plans.
+//
+// Reference loop nest (triangle, order [a,b,c]; EHGenerator.scala:273-480,
+// TrieBuilder.cpp:242-274, ParTrieBuilder::par_foreach_aggregate
+// TrieBuilder.hpp:152-157):
+//     for a in head ∩ head (parallel, par::for_range chunks):
+//       for b in N(a) ∩ head:
+//         count += |N(b) ∩ N(a)|          (ops::set_intersect, set.hpp:9-167)
+// The same pairwise intersections are scheduled here grouped by b: N(b) is
+// staged once in shared memory in its stored layout (uint -> sorted list,
+// range bitset -> words, block bitset -> ids + words) and every row a->b
+// streams the part of N(a) that can still meet N(b) (the reverse level of
+// the trie, built with it).  The sum is unchanged: it is the same set of
+// (a,b) intersections.  Work items are (b, range of rows a->b) chunks of
+// about `chunk_pairs` probes, pulled by warps of a persistent kernel from
+// an atomic queue, heaviest b first.
+#include <algorithm>
+
+#include "eh_internal.cuh"
+
+namespace eh {
+
+constexpr int kDefaultWarps = 8;
+constexpr int kDefaultSmemWords = 2048;  // per warp: 8 KB
+constexpr int kDefaultChunk = 8192;
+
+struct RevView {
+  const uint64_t* rev_off;
+  const uint32_t* rev_lo;
+  const uint32_t* rev_hi;
+  const uint32_t* rev_src;
+  const uint64_t* rev_wpre;
+  int dir;
+};
+
+struct Item {  // 16 bytes
+  uint32_t hb, kb, ke, g;
+};
+
+struct ExecParams {
+  int warps;
+  int smem_words;
+  uint32_t chunk;
+  uint32_t shard_index, shard_count;
+};
+
+static ExecParams exec_params(const eh_exec_config* cfg) {
+  ExecParams p;
+  p.warps = (cfg && cfg->warps_per_block > 0) ? cfg->warps_per_block : kDefaultWarps;
+  p.smem_words = (cfg && cfg->smem_words > 0) ? cfg->smem_words : kDefaultSmemWords;
+  p.chunk = (cfg && cfg->chunk_pairs > 0) ? (uint32_t)cfg->chunk_pairs : (uint32_t)kDefaultChunk;
+  p.shard_count = (cfg && cfg->shard_count > 1) ? (uint32_t)cfg->shard_count : 1u;
+  p.shard_index = (cfg && cfg->shard_count > 1) ? (uint32_t)cfg->shard_index : 0u;
+  EH_REQUIRE(p.shard_index < p.shard_count, EH_ERR_INVALID, "shard_index must be below shard_count");
+  p.warps = std::max(1, std::min(p.warps, 32));
+  p.smem_words = std::max(64, std::min(p.smem_words, 16384)) & ~1;
+  return p;
+}
+
+// ---------------------------------------------------------------- planning
+// items per head entry b: ceil(work(b) / chunk)
+__global__ void plan_count_kernel(RevView r, uint32_t nh, uint32_t chunk, uint32_t* __restrict__ nitems) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nh; b += gridDim.x * blockDim.x) {
+    const uint64_t w = r.rev_wpre[r.rev_off[b + 1]] - r.rev_wpre[r.rev_off[b]];
+    nitems[b] = (uint32_t)((w + chunk - 1) / chunk);
+  }
+}
+// item i of b covers the rows whose work prefix falls in [i, i+1) * W/n;
+// items are written in reverse head order so the queue starts at the
+// largest-degree b (ids are degree-ordered) and small items come last
+__global__ void plan_fill_kernel(RevView r, uint32_t nh, const uint32_t* __restrict__ nitems,
+                                 const uint32_t* __restrict__ ipos, uint32_t total, uint32_t g,
+                                 Item* __restrict__ items) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nh; b += gridDim.x * blockDim.x) {
+    const uint32_t n = nitems[b];
+    if (!n) continue;
+    const uint64_t k0 = r.rev_off[b], k1 = r.rev_off[b + 1];
+    const uint64_t w0 = r.rev_wpre[k0], W = r.rev_wpre[k1] - w0;
+    uint64_t kb = k0;
+    for (uint32_t i = 0; i < n; i++) {
+      uint64_t ke = k1;
+      if (i + 1 < n) {
+        const uint64_t target = w0 + (W * (i + 1)) / n;
+        uint64_t lo = kb, hi = k1;  // first k with wpre[k] >= target
+        while (lo < hi) {
+          const uint64_t mid = (lo + hi) >> 1;
+          if (r.rev_wpre[mid] < target) lo = mid + 1; else hi = mid;
+        }
+        ke = lo;
+      }
+      if (ke > kb) items[total - 1 - (ipos[b] + i)] = Item{b, (uint32_t)kb, (uint32_t)ke, g};
+      else items[total - 1 - (ipos[b] + i)] = Item{b, (uint32_t)kb, (uint32_t)kb, g};
+      kb = ke;
+    }
+  }
+}
+
+struct Plan {
+  DevBuf<Item> items;
+  uint32_t n = 0;
+};
+
+static void build_plan(eh_context* ctx, const eh_trie* t, uint32_t chunk, uint32_t g, Plan& plan) {
+  cudaStream_t s = ctx->stream;
+  plan.n = 0;
+  if (!t->rev_entries) return;
+  RevView r{t->rev_off.p, t->rev_lo.p, t->rev_hi.p, t->rev_src.p, t->rev_wpre.p, t->dir};
+  DevBuf<uint32_t> nitems(t->n_head, s), ipos(t->n_head, s), tot(1, s);
+  const int grid = num_sms() * 4;
+  plan_count_kernel<<<grid, 256, 0, s>>>(r, t->n_head, chunk, nitems.p);
+  EH_CHECK_LAUNCH();
+  exclusive_scan<uint32_t>(nitems.p, ipos.p, t->n_head, tot.p, s);
+  uint32_t n = 0;
+  EH_CUDA(cudaMemcpyAsync(&n, tot.p, 4, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaStreamSynchronize(s));
+  plan.items.alloc(n ? n : 1, s);
+  plan.n = n;
+  if (n) {
+    plan_fill_kernel<<<grid, 256, 0, s>>>(r, t->n_head, nitems.p, ipos.p, n, g, plan.items.p);
+    EH_CHECK_LAUNCH();
+  }
+}
+
+// ------------------------------------------------------------------ probes
+// Probe structures for the staged set N(b), one per stored layout.
+enum { P_SBITS = 0, P_GBITS = 1, P_SLIST = 2, P_GLIST = 3, P_GBLOCK = 4 };
+
+struct Staged {
+  const uint64_t* words;  // P_SBITS (shared) / P_GBITS (global)
+  const uint32_t* list;   // P_SLIST (shared) / P_GLIST (global)
+  const uint32_t* ids;    // P_GBLOCK
+  const uint64_t* bwords; // P_GBLOCK
+  uint32_t start;         // first word index (bitsets)
+  uint32_t n;             // words / list length / blocks
+};
+
+// branch-free lower bound over a sorted run of n >= 1 values
+template <bool kShared>
+__device__ __forceinline__ bool list_contains(const uint32_t* p, uint32_t n, uint32_t w) {
+  uint32_t base = 0;
+  while (n > 1) {
+    const uint32_t half = n >> 1;
+    const uint32_t v = kShared ? p[base + half] : __ldg(p + base + half);
+    base = (v <= w) ? base + half : base;
+    n -= half;
+  }
+  return (kShared ? p[base] : __ldg(p + base)) == w;
+}
+
+template <int P>
+__device__ __forceinline__ uint32_t probe(const Staged& s, uint32_t w) {
+  if (P == P_SBITS || P == P_GBITS) {
+    const uint32_t idx = (w >> 6) - s.start;
+    if (idx >= s.n) return 0;  // also catches w below the first word (wraps)
+    const uint64_t word = (P == P_SBITS) ? s.words[idx] : __ldg(s.words + idx);
+    return (uint32_t)(word >> (w & 63)) & 1u;
+  } else if (P == P_SLIST || P == P_GLIST) {
+    return list_contains<P == P_SLIST>(s.list, s.n, w) ? 1u : 0u;
+  } else {  // block bitset: find block id w >> 8, test its word
+    const uint32_t id = w >> 8;
+    uint32_t lo = 0, hi = s.n;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (__ldg(s.ids + mid) < id) lo = mid + 1; else hi = mid;
+    }
+    if (lo >= s.n || __ldg(s.ids + lo) != id) return 0;
+    return (uint32_t)(__ldg(s.bwords + 4 * (uint64_t)lo + ((w >> 6) & 3)) >> (w & 63)) & 1u;
+  }
+}
+
+// Stream the candidate ranges of rows [kb, ke) against the staged set,
+// flattening (row, element) pairs over the 32 lanes.  kAnnot adds each
+// hit to the annotation of the row's source (and, for symmetric tries,
+// of the matched element).
+template <int P, bool kAnnot>
+__device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView& t, const RevView& r, uint32_t kb,
+                                                uint32_t ke, unsigned long long* annot) {
+  const uint32_t lane = lane_id();
+  uint64_t cnt = 0;
+  for (uint32_t k0 = kb; k0 < ke; k0 += 32) {
+    const uint32_t k = k0 + lane;
+    uint32_t lo = 0, len = 0, src = 0;
+    if (k < ke) {
+      lo = __ldg(r.rev_lo + k);
+      len = __ldg(r.rev_hi + k) - lo;
+      if (kAnnot) src = __ldg(r.rev_src + k);
+    }
+    const uint32_t incl = warp_incl_scan(len);
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    const uint32_t excl = incl - len;
+    for (uint32_t p = 0; p < total; p += 32) {
+      const uint32_t q = p + lane;
+      uint32_t j = 0;
+#pragma unroll
+      for (int step = 16; step; step >>= 1) {
+        const uint32_t tj = __shfl_sync(kFull, incl, j + step - 1);
+        if (tj <= q) j += step;
+      }
+      const uint32_t lo_j = __shfl_sync(kFull, lo, j);
+      const uint32_t ex_j = __shfl_sync(kFull, excl, j);
+      uint32_t src_j = 0;
+      if (kAnnot) src_j = __shfl_sync(kFull, src, j);
+      if (q < total) {
+        const uint32_t w = __ldg(t.vals + lo_j + (q - ex_j));
+        const uint32_t hit = probe<P>(st, w);
+        cnt += hit;
+        if (kAnnot && hit) {
+          if (r.dir == DIR_SYM) {
+            atomicAdd(annot + src_j, 2ull);
+            atomicAdd(annot + __ldg(t.head_index + w), 2ull);
+          } else {
+            atomicAdd(annot + src_j, 1ull);
+          }
+        }
+      }
+    }
+  }
+  return cnt;
+}
+
+// Stage N(b) in the warp's shared region according to its layout; returns
+// the probe mode.
+__device__ __forceinline__ int stage_set(const TrieView& t, uint32_t hb, uint32_t* sm, int cap_words, Staged& st) {
+  const uint32_t lane = lane_id();
+  const uint8_t layout = t.layout[hb];
+  const SetAux a = t.aux[hb];
+  const uint64_t s0 = t.off[hb];
+  const uint32_t len = (uint32_t)(t.off[hb + 1] - s0);
+  if (layout == EH_LAYOUT_RANGE_BITSET) {
+    st.start = a.start;
+    st.n = a.n;
+    if (2 * a.n <= (uint32_t)cap_words) {
+      uint64_t* sw = reinterpret_cast<uint64_t*>(sm);
+      for (uint32_t j = lane; j < a.n; j += 32) sw[j] = __ldg(t.bs_words + a.off + j);
+      __syncwarp();
+      st.words = sw;
+      return P_SBITS;
+    }
+    st.words = t.bs_words + a.off;
+    return P_GBITS;
+  }
+  if (layout == EH_LAYOUT_BLOCK_BITSET) {
+    st.ids = t.bb_id + a.off;
+    st.bwords = t.bb_words + 4 * a.off;
+    st.n = a.n;
+    return P_GBLOCK;
+  }
+  st.n = len;
+  if (len <= (uint32_t)cap_words) {
+    for (uint32_t j = lane; j < len; j += 32) sm[j] = __ldg(t.vals + s0 + j);
+    __syncwarp();
+    st.list = sm;
+    return P_SLIST;
+  }
+  st.list = t.vals + s0;
+  return P_GLIST;
+}
+
+struct QueryOut {
+  uint32_t shard_index, shard_count;  // this launch runs items shard_index + q * shard_count
+  unsigned long long* total;   // per graph results (one per trie)
+  unsigned long long* annot;   // per head entry annotation or null
+  float* records;              // per item timing records or null
+  unsigned int* queue;         // atomic queue head
+  unsigned int* error;         // set when a bound is hit
+};
+
+template <bool kAnnot>
+__global__ void __launch_bounds__(1024) triangle_kernel(const TrieView* __restrict__ views,
+                                                        const RevView* __restrict__ revs,
+                                                        const Item* __restrict__ items, uint32_t n_items,
+                                                        int cap_words, QueryOut out) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t lane = lane_id();
+  const uint32_t wid = threadIdx.x >> 5;
+  uint32_t* sm = smem + (size_t)wid * cap_words;
+  unsigned long long acc = 0;
+  uint32_t cur_g = 0xffffffffu;
+  for (;;) {
+    uint32_t q = 0;
+    if (lane == 0) q = atomicAdd(out.queue, 1u);
+    q = __shfl_sync(kFull, q, 0);
+    const uint64_t it64 = (uint64_t)out.shard_index + (uint64_t)q * out.shard_count;
+    if (it64 >= n_items) break;
+    const uint32_t it = (uint32_t)it64;
+    const Item item = items[it];
+    if (item.g != cur_g) {  // flush the running count of the previous graph
+      if (lane == 0 && cur_g != 0xffffffffu && acc) atomicAdd(out.total + cur_g, acc);
+      acc = 0;
+      cur_g = item.g;
+    }
+    const TrieView t = views[item.g];
+    const RevView r = revs[item.g];
+    long long t0 = 0;
+    if (out.records && lane == 0) t0 = clock64();
+    Staged st;
+    const int mode = stage_set(t, item.hb, sm, cap_words, st);
+    unsigned long long* annot = kAnnot ? out.annot : nullptr;
+    uint64_t c;
+    switch (mode) {
+      case P_SBITS: c = stream_rows<P_SBITS, kAnnot>(st, t, r, item.kb, item.ke, annot); break;
+      case P_GBITS: c = stream_rows<P_GBITS, kAnnot>(st, t, r, item.kb, item.ke, annot); break;
+      case P_SLIST: c = stream_rows<P_SLIST, kAnnot>(st, t, r, item.kb, item.ke, annot); break;
+      case P_GLIST: c = stream_rows<P_GLIST, kAnnot>(st, t, r, item.kb, item.ke, annot); break;
+      default: c = stream_rows<P_GBLOCK, kAnnot>(st, t, r, item.kb, item.ke, annot); break;
+    }
+    c = warp_sum(c);
+    if (kAnnot && r.dir == DIR_SYM && lane == 0 && c) atomicAdd(out.annot + item.hb, 2ull * c);
+    acc += c;
+    __syncwarp();  // the staged region is reused by the next item
+    if (out.records && lane == 0) {
+      const long long t1 = clock64();
+      const uint32_t len = (uint32_t)(t.off[item.hb + 1] - t.off[item.hb]);
+      const uint64_t pairs = r.rev_wpre[item.ke] - r.rev_wpre[item.kb];
+      const uint32_t first = t.vals[t.off[item.hb]], last = t.vals[t.off[item.hb + 1] - 1];
+      float* rec = out.records + 8 * (size_t)it;
+      rec[0] = (float)len;
+      rec[1] = (float)pairs;
+      rec[2] = (float)len / (float)(last - first + 1);
+      rec[3] = (float)(last - first);
+      rec[4] = (float)t.layout[item.hb];
+      rec[5] = (float)mode;
+      rec[6] = __uint_as_float(item.hb);  // set id, bit pattern
+      rec[7] = (float)(t1 - t0);
+    }
+  }
+  if (lane == 0 && cur_g != 0xffffffffu && acc) atomicAdd(out.total + cur_g, acc);
+}
+
+// ------------------------------------------------------------ 4-clique
+// For every row a->b (UP / DOWN / SYM-oriented): S = candidates(a,b) ∩ N(b)
+// is materialised in the warp's shared region, then for each c in S the
+// elements of S on the far side of c are probed in N(c).
+__device__ __forceinline__ uint32_t probe_global_set(const TrieView& t, uint32_t hc, uint32_t w) {
+  const uint8_t layout = t.layout[hc];
+  const SetAux a = t.aux[hc];
+  if (layout == EH_LAYOUT_RANGE_BITSET) {
+    Staged st;
+    st.words = t.bs_words + a.off;
+    st.start = a.start;
+    st.n = a.n;
+    return probe<P_GBITS>(st, w);
+  }
+  if (layout == EH_LAYOUT_BLOCK_BITSET) {
+    Staged st;
+    st.ids = t.bb_id + a.off;
+    st.bwords = t.bb_words + 4 * a.off;
+    st.n = a.n;
+    return probe<P_GBLOCK>(st, w);
+  }
+  const uint64_t s0 = t.off[hc];
+  const uint32_t n = (uint32_t)(t.off[hc + 1] - s0);
+  if (!n) return 0;
+  return list_contains<false>(t.vals + s0, n, w) ? 1u : 0u;
+}
+
+template <int P>
+__device__ uint64_t clique_rows(const Staged& st, const TrieView& t, const RevView& r, uint32_t kb, uint32_t ke,
+                                uint32_t* sbuf, uint32_t cap) {
+  const uint32_t lane = lane_id();
+  const bool up = r.dir != DIR_DOWN;
+  uint64_t cnt = 0;
+  for (uint32_t k = kb; k < ke; k++) {
+    const uint32_t lo = __ldg(r.rev_lo + k), hi = __ldg(r.rev_hi + k);
+    // S = N(a)[lo, hi) ∩ N(b), compacted in order
+    uint32_t ns = 0;
+    for (uint32_t base = lo; base < hi; base += 32) {
+      const uint32_t e = base + lane;
+      uint32_t w = 0, hit = 0;
+      if (e < hi) {
+        w = __ldg(t.vals + e);
+        hit = probe<P>(st, w);
+      }
+      const uint32_t ball = __ballot_sync(kFull, hit);
+      if (hit) {
+        const uint32_t pos = ns + __popc(ball & lanemask_lt());
+        if (pos < cap) sbuf[pos] = w;
+      }
+      ns += __popc(ball);
+    }
+    __syncwarp();
+    if (ns > cap) ns = cap;  // capacity bound checked by the host planner
+    // for each c = S[i]: count S elements beyond c (up) or before c (down) in N(c)
+    for (uint32_t i = 0; i < ns; i++) {
+      const uint32_t c = sbuf[i];
+      const int32_t hc = __ldg(t.head_index + c);
+      if (hc < 0) continue;
+      const uint32_t jb = up ? i + 1 : 0, je = up ? ns : i;
+      for (uint32_t j = jb + lane; j < je; j += 32) cnt += probe_global_set(t, (uint32_t)hc, sbuf[j]);
+    }
+    __syncwarp();
+  }
+  return cnt;
+}
+
+__global__ void __launch_bounds__(1024) clique4_kernel(const TrieView* __restrict__ views,
+                                                       const RevView* __restrict__ revs,
+                                                       const Item* __restrict__ items, uint32_t n_items,
+                                                       int cap_words, QueryOut out) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t lane = lane_id();
+  const uint32_t wid = threadIdx.x >> 5;
+  uint32_t* sm = smem + (size_t)wid * cap_words;
+  const int half = cap_words / 2;
+  unsigned long long acc = 0;
+  uint32_t cur_g = 0xffffffffu;
+  for (;;) {
+    uint32_t q = 0;
+    if (lane == 0) q = atomicAdd(out.queue, 1u);
+    q = __shfl_sync(kFull, q, 0);
+    const uint64_t it64 = (uint64_t)out.shard_index + (uint64_t)q * out.shard_count;
+    if (it64 >= n_items) break;
+    const uint32_t it = (uint32_t)it64;
+    const Item item = items[it];
+    if (item.g != cur_g) {
+      if (lane == 0 && cur_g != 0xffffffffu && acc) atomicAdd(out.total + cur_g, acc);
+      acc = 0;
+      cur_g = item.g;
+    }
+    const TrieView t = views[item.g];
+    const RevView r = revs[item.g];
+    Staged st;
+    const int mode = stage_set(t, item.hb, sm, half, st);
+    uint32_t* sbuf = sm + half;
+    uint64_t c;
+    switch (mode) {
+      case P_SBITS: c = clique_rows<P_SBITS>(st, t, r, item.kb, item.ke, sbuf, half); break;
+      case P_GBITS: c = clique_rows<P_GBITS>(st, t, r, item.kb, item.ke, sbuf, half); break;
+      case P_SLIST: c = clique_rows<P_SLIST>(st, t, r, item.kb, item.ke, sbuf, half); break;
+      case P_GLIST: c = clique_rows<P_GLIST>(st, t, r, item.kb, item.ke, sbuf, half); break;
+      default: c = clique_rows<P_GBLOCK>(st, t, r, item.kb, item.ke, sbuf, half); break;
+    }
+    acc += warp_sum(c);
+    __syncwarp();
+  }
+  if (lane == 0 && cur_g != 0xffffffffu && acc) atomicAdd(out.total + cur_g, acc);
+}
+
+// ------------------------------------------------- lollipop / barbell roots
+// LollipopAgg root, order [a,d]: sum_a T(a) * |N(a)|
+// BarbellAgg root, order [a,x]: sum_a T(a) * sum_{x in N(a) ∩ head} T(x)
+template <bool kBarbell>
+__global__ void root_kernel(TrieView t, const unsigned long long* __restrict__ T,
+                            unsigned long long* __restrict__ total) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  unsigned long long acc = 0;
+  for (uint32_t a = warp; a < t.n_head; a += nwarps) {
+    const unsigned long long ta = T[a];
+    if (!ta) continue;
+    unsigned long long s = 0;
+    if (kBarbell) {
+      for (uint64_t e = t.off[a] + lane; e < t.off[a + 1]; e += 32) {
+        const int32_t hx = __ldg(t.head_index + __ldg(t.vals + e));
+        if (hx >= 0) s += T[hx];
+      }
+      s = warp_sum(s);
+    } else {
+      s = t.off[a + 1] - t.off[a];
+    }
+    acc += ta * s;
+  }
+  if (lane == 0 && acc) atomicAdd(total, acc);
+}
+
+// ---------------------------------------------------------------- driver
+static RevView rev_view(const eh_trie* t) {
+  return RevView{t->rev_off.p, t->rev_lo.p, t->rev_hi.p, t->rev_src.p, t->rev_wpre.p, t->dir};
+}
+
+static int blocks_per_sm(const void* kernel, int threads, size_t smem) {
+  int b = 0;
+  EH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, smem));
+  return std::max(1, b);
+}
+
+template <typename K>
+static void set_smem_attr(K kernel, size_t smem) {
+  EH_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+}
+
+struct Launch {
+  uint32_t launches = 0;
+  float kernel_ms = 0;
+};
+
+// Runs the intersection kernel of `query` over the concatenated plans of
+// n graphs; results accumulate into d_total[g].
+static Launch run_plans(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query, const ExecParams& ep,
+                        bool annot, unsigned long long* d_total, unsigned long long* d_annot, float* d_records,
+                        uint32_t* n_items_out, uint64_t* pairs_out) {
+  cudaStream_t s = ctx->stream;
+  Launch L;
+  std::vector<Plan> plans(n);
+  uint32_t total_items = 0;
+  uint64_t pairs = 0;
+  for (uint32_t g = 0; g < n; g++) {
+    build_plan(ctx, tries[g], ep.chunk, g, plans[g]);
+    L.launches += plans[g].n ? 2 : 1;
+    total_items += plans[g].n;
+    pairs += tries[g]->rev_pairs;
+  }
+  *n_items_out = total_items;
+  *pairs_out = pairs;
+  if (!total_items) return L;
+  DevBuf<Item> items;
+  const Item* items_p = plans[0].items.p;
+  if (n > 1) {
+    items.alloc(total_items, s);
+    uint32_t o = 0;
+    for (uint32_t g = 0; g < n; g++) {
+      if (plans[g].n)
+        EH_CUDA(cudaMemcpyAsync(items.p + o, plans[g].items.p, plans[g].n * sizeof(Item), cudaMemcpyDeviceToDevice, s));
+      o += plans[g].n;
+    }
+    items_p = items.p;
+  }
+  std::vector<TrieView> hv(n);
+  std::vector<RevView> hr(n);
+  for (uint32_t g = 0; g < n; g++) {
+    hv[g] = tries[g]->view();
+    hr[g] = rev_view(tries[g]);
+  }
+  DevBuf<TrieView> dv(n, s);
+  DevBuf<RevView> dr(n, s);
+  DevBuf<unsigned int> q(2, s);
+  EH_CUDA(cudaMemcpyAsync(dv.p, hv.data(), n * sizeof(TrieView), cudaMemcpyHostToDevice, s));
+  EH_CUDA(cudaMemcpyAsync(dr.p, hr.data(), n * sizeof(RevView), cudaMemcpyHostToDevice, s));
+  EH_CUDA(cudaMemsetAsync(q.p, 0, 8, s));
+  QueryOut out{ep.shard_index, ep.shard_count, d_total, d_annot, d_records, q.p, q.p + 1};
+  const int threads = 32 * ep.warps;
+  const size_t smem = (size_t)ep.smem_words * 4 * ep.warps;
+  const void* kfn;
+  if (query == EH_QUERY_CLIQUE4) {
+    set_smem_attr(clique4_kernel, smem);
+    kfn = (const void*)clique4_kernel;
+  } else if (annot) {
+    set_smem_attr(triangle_kernel<true>, smem);
+    kfn = (const void*)triangle_kernel<true>;
+  } else {
+    set_smem_attr(triangle_kernel<false>, smem);
+    kfn = (const void*)triangle_kernel<false>;
+  }
+  const int per_sm = blocks_per_sm(kfn, threads, smem);
+  const int warps_total = num_sms() * per_sm * ep.warps;
+  const int grid = std::max(1, std::min(num_sms() * per_sm, (int)((total_items + ep.warps - 1) / ep.warps)));
+  (void)warps_total;
+  EH_CUDA(cudaEventRecord(ctx->ev1, s));
+  if (query == EH_QUERY_CLIQUE4)
+    clique4_kernel<<<grid, threads, smem, s>>>(dv.p, dr.p, items_p, total_items, ep.smem_words, out);
+  else if (annot)
+    triangle_kernel<true><<<grid, threads, smem, s>>>(dv.p, dr.p, items_p, total_items, ep.smem_words, out);
+  else
+    triangle_kernel<false><<<grid, threads, smem, s>>>(dv.p, dr.p, items_p, total_items, ep.smem_words, out);
+  EH_CHECK_LAUNCH();
+  EH_CUDA(cudaEventRecord(ctx->ev2, s));
+  L.launches += 1;
+  EH_CUDA(cudaEventSynchronize(ctx->ev2));
+  EH_CUDA(cudaEventElapsedTime(&L.kernel_ms, ctx->ev1, ctx->ev2));
+  return L;
+}
+
+// Algorithmic bytes of the triangle plan: both uint32 inputs of every
+// pairwise intersection the reference loop nest evaluates, read once each:
+// 4 * sum over rows (a,b) of (d(a) + d(b)) = 4 * (sum_a d(a)^2 + wedges).
+static uint64_t triangle_algorithmic_bytes(const eh_trie* t) { return 4 * (t->sum_sq_deg + t->total_wedges); }
+
+static void fill_stats(eh_query_stats* st, float query_ms, const Launch& L, uint32_t items, uint64_t pairs,
+                       uint64_t alg) {
+  if (!st) return;
+  st->query_ms = query_ms;
+  st->kernel_ms = L.kernel_ms;
+  st->launches = L.launches;
+  st->work_items = items;
+  st->wedges = pairs;
+  st->algorithmic_bytes = alg;
+  st->timed_out = 0;
+}
+
+void query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query,
+                         const eh_exec_config* cfg, uint64_t* results, eh_query_stats* stats) {
+  cudaStream_t s = ctx->stream;
+  EH_REQUIRE(query >= EH_QUERY_TRIANGLE && query <= EH_QUERY_BARBELL, EH_ERR_INVALID, "unknown query");
+  EH_REQUIRE(n > 0, EH_ERR_INVALID, "no tries");
+  for (uint32_t g = 0; g < n; g++) {
+    EH_REQUIRE(tries[g] != nullptr, EH_ERR_INVALID, "null trie");
+    EH_REQUIRE(tries[g]->ctx == ctx, EH_ERR_INVALID, "trie belongs to another context");
+  }
+  if (query == EH_QUERY_CLIQUE4)
+    for (uint32_t g = 0; g < n; g++)
+      EH_REQUIRE(tries[g]->dir != DIR_GENERAL || tries[g]->rows == 0, EH_ERR_UNSUPPORTED,
+                 "4-clique needs a relation that is up-, down-oriented or symmetric");
+  ExecParams ep = exec_params(cfg);
+  if (query == EH_QUERY_CLIQUE4) {
+    // the warp's region holds the staged set and S (<= the largest set)
+    uint32_t mx = 0;
+    for (uint32_t g = 0; g < n; g++) mx = std::max(mx, tries[g]->info.max_set);
+    const int need = 2 * ((int)mx + 1);
+    if (ep.smem_words < need) ep.smem_words = (need + 1) & ~1;
+    EH_REQUIRE((size_t)ep.smem_words * 4 * ep.warps <= 200 * 1024, EH_ERR_UNSUPPORTED,
+               "4-clique: largest set too large for the shared-memory staging");
+  }
+  EH_CUDA(cudaEventRecord(ctx->ev0, s));
+  DevBuf<unsigned long long> total(n, s);
+  EH_CUDA(cudaMemsetAsync(total.p, 0, n * 8, s));
+  uint32_t items = 0;
+  uint64_t pairs = 0;
+  Launch L;
+  DevBuf<float> rec;
+  const bool record = cfg && cfg->record_timings && n == 1;
+  if (query == EH_QUERY_TRIANGLE || query == EH_QUERY_CLIQUE4) {
+    float* recp = nullptr;
+    if (record) {
+      // one record per item; the plan size is known only after planning, so
+      // size for the worst case of one item per head entry plus splits
+      const uint64_t cap = tries[0]->n_head + tries[0]->rev_pairs / ep.chunk + 16;
+      rec.alloc(8 * cap, s);
+      recp = rec.p;
+    }
+    L = run_plans(ctx, tries, n, query, ep, false, total.p, nullptr, recp, &items, &pairs);
+  } else {
+    EH_REQUIRE(n == 1, EH_ERR_UNSUPPORTED, "batched lollipop/barbell is not supported");
+    const eh_trie* t = tries[0];
+    EH_REQUIRE(ep.shard_count == 1, EH_ERR_UNSUPPORTED, "lollipop/barbell run unsharded");
+    DevBuf<unsigned long long> T(t->n_head ? t->n_head : 1, s), dummy(1, s);
+    EH_CUDA(cudaMemsetAsync(T.p, 0, (t->n_head ? t->n_head : 1) * 8, s));
+    EH_CUDA(cudaMemsetAsync(dummy.p, 0, 8, s));
+    L = run_plans(ctx, tries, 1, EH_QUERY_TRIANGLE, ep, true, dummy.p, T.p, nullptr, &items, &pairs);
+    if (t->n_head) {
+      if (query == EH_QUERY_LOLLIPOP)
+        root_kernel<false><<<num_sms() * 8, 256, 0, s>>>(t->view(), T.p, total.p);
+      else
+        root_kernel<true><<<num_sms() * 8, 256, 0, s>>>(t->view(), T.p, total.p);
+      EH_CHECK_LAUNCH();
+      L.launches++;
+    }
+  }
+  std::vector<unsigned long long> h(n);
+  EH_CUDA(cudaMemcpyAsync(h.data(), total.p, n * 8, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaEventRecord(ctx->ev2, s));
+  EH_CUDA(cudaEventSynchronize(ctx->ev2));
+  float qms = 0;
+  EH_CUDA(cudaEventElapsedTime(&qms, ctx->ev0, ctx->ev2));
+  for (uint32_t g = 0; g < n; g++) {
+    uint64_t v = h[g];
+    const int dir = tries[g]->dir;
+    // on a symmetric relation every undirected triangle is found once (rows
+    // a<b) and the reference counts each of its 3! orderings; 4! for 4-cliques
+    if (dir == DIR_SYM && query == EH_QUERY_TRIANGLE) v *= 6ull;
+    if (dir == DIR_SYM && query == EH_QUERY_CLIQUE4) v *= 24ull;
+    results[g] = v;
+  }
+  if (record) {
+    ctx->timing_records.resize(8 * (size_t)items);
+    if (items)
+      EH_CUDA(cudaMemcpy(ctx->timing_records.data(), rec.p, 8 * (size_t)items * sizeof(float), cudaMemcpyDeviceToHost));
+  }
+  uint64_t alg = 0;
+  for (uint32_t g = 0; g < n; g++) alg += triangle_algorithmic_bytes(tries[g]);
+  fill_stats(stats, qms, L, items, pairs, alg);
+}
+
+void query_count(eh_context* ctx, const eh_trie* t, int query, const eh_exec_config* cfg, uint64_t* result,
+                 eh_query_stats* stats) {
+  const eh_trie* ts[1] = {t};
+  query_count_batched(ctx, ts, 1, query, cfg, result, stats);
+}
+
+void triangle_annotation(eh_context* ctx, const eh_trie* t, const eh_exec_config* cfg, uint64_t* annot_dev) {
+  cudaStream_t s = ctx->stream;
+  ExecParams ep = exec_params(cfg);
+  ep.shard_index = 0;
+  ep.shard_count = 1;
+  DevBuf<unsigned long long> dummy(1, s);
+  EH_CUDA(cudaMemsetAsync(annot_dev, 0, (t->n_head ? t->n_head : 1) * 8, s));
+  EH_CUDA(cudaMemsetAsync(dummy.p, 0, 8, s));
+  uint32_t items;
+  uint64_t pairs;
+  const eh_trie* ts[1] = {t};
+  run_plans(ctx, ts, 1, EH_QUERY_TRIANGLE, ep, true, dummy.p, (unsigned long long*)annot_dev, nullptr, &items,
+            &pairs);
+  EH_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace eh

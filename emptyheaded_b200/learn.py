@@ -1,0 +1,150 @@
+"""Learned layout policy: profile, train, evaluate.
+
+The engine logs, for every work item of a triangle query, the SM cycles it
+spent on the staged set N(b) under the layout that set had
+(eh_timing_records).  `profile` runs the query once per candidate layout
+(uint / range bitset / block bitset, each set forced where admissible) and
+sums the cycles per set: for every set this is an exhaustive layout search.
+`train` fits the cost model (the engine's fp32 MLP, trained on the GPU by
+its own kernels) to predict log cycles from the set's features and a
+layout; EH_POLICY_LEARNED then gives each set its predicted-cheapest
+layout.  The reference's density rule (common::is_sparse,
+utils/common.hpp:60-66) stays as the fallback for sets the plan never
+stages and as the judge: `evaluate` reports the model's prediction error
+and the regret of both policies against the exhaustive search.
+"""
+import numpy as np
+
+UINT, BITSET, BLOCK = 1, 0, 3
+LAYOUTS = (UINT, BITSET, BLOCK)
+DIMS = [6, 32, 32, 1]
+# per-set cap used when forcing range bitsets for profiling: the same
+# admission the learned chooser applies (16 words per element + 64)
+REL_WORDS, ABS_WORDS = 16, 64
+
+
+def set_features(head_len, rng, pairs, layout):
+    """Features of a set for the model (fp32): log1p(len), log1p(range),
+    density len/(range+1), log1p(pairs probed against it), layout one-hot
+    (bitset, block); uint is the zero vector.  Matches model_features in
+    csrc/eh_model.cu."""
+    f = np.zeros((len(head_len), 6), np.float32)
+    f[:, 0] = np.log1p(head_len)
+    f[:, 1] = np.log1p(rng)
+    f[:, 2] = head_len / (rng + 1.0)
+    f[:, 3] = np.log1p(pairs)
+    f[:, 4] = layout == BITSET
+    f[:, 5] = layout == BLOCK
+    return f
+
+
+def profile(E, trie, reps=2):
+    """Per-set cycles under each layout.  Returns (len, range, pairs,
+    cycles[layout] with NaN where the layout was not admissible, base
+    heuristic layout)."""
+    head, off, vals, heur = trie.export()
+    n = len(head)
+    lens = np.diff(off).astype(np.float64)
+    first = vals[off[:-1].astype(np.int64)].astype(np.float64)
+    last = vals[np.maximum(off[1:].astype(np.int64) - 1, 0)].astype(np.float64)
+    rng = np.where(lens > 0, last - first, 0.0)
+    words = np.floor(last / 64) - np.floor(first / 64) + 1
+    cycles = {}
+    pairs = np.zeros(n)
+    for L in LAYOUTS:
+        if L == BITSET:
+            # admission per set as in the learned chooser (16 words per
+            # element + 64); the absolute cap is set out of the way
+            trie.relayout(policy=E.FORCED, forced=BITSET, max_bitset_bytes=1 << 50)
+            ok = words <= REL_WORDS * lens + ABS_WORDS
+        else:
+            trie.relayout(policy=E.FORCED, forced=L)
+            ok = np.ones(n, bool)
+        _, _, _, lay = trie.export()
+        acc = np.zeros(n)
+        for _ in range(reps):
+            trie.count("triangle", record=True)
+            rec = E.timing_records(trie.ctx)
+            hb = rec[:, 6].view(np.uint32).astype(np.int64)
+            acc += np.bincount(hb, weights=rec[:, 7].astype(np.float64), minlength=n)
+            pairs = np.bincount(hb, weights=rec[:, 1].astype(np.float64), minlength=n)
+        c = acc / reps
+        c[(lay != L) | ~ok] = np.nan
+        cycles[L] = c
+    trie.relayout()
+    return dict(lens=lens, range=rng, pairs=pairs, cycles=cycles, heuristic=heur.astype(np.int64), words=words)
+
+
+def dataset(prof):
+    xs, ys = [], []
+    staged = prof["pairs"] > 0
+    for L in LAYOUTS:
+        c = prof["cycles"][L]
+        m = staged & np.isfinite(c) & (c > 0)
+        xs.append(set_features(prof["lens"][m], prof["range"][m], prof["pairs"][m], np.full(m.sum(), L)))
+        ys.append(np.log1p(c[m]).astype(np.float32)[:, None])
+    return np.concatenate(xs), np.concatenate(ys)
+
+
+def train(E, x, y, ctx=None, epochs=60, batch=4096, lr=0.02, seed=0):
+    """SGD on the device (eh_model_train) over shuffled minibatches."""
+    model = E.Model(DIMS, seed=seed, ctx=ctx)
+    mu = float(y.mean())
+    # start the output bias at the mean target so SGD fits the residual
+    p = model.params()
+    p[-1] = mu
+    model.set_params(p)
+    rng = np.random.default_rng(seed)
+    n = len(x)
+    losses = []
+    for ep in range(epochs):
+        perm = rng.permutation(n)
+        for i in range(0, n, batch):
+            idx = perm[i:i + batch]
+            if len(idx) < 16:
+                continue
+            losses.append(model.train(x[idx], y[idx], lr=lr, steps=1))
+    return model, losses
+
+
+def evaluate(E, model, prof):
+    """Prediction error and regret against the per-set exhaustive search."""
+    staged = prof["pairs"] > 0
+    n = len(prof["lens"])
+    C = np.stack([prof["cycles"][L] for L in LAYOUTS], 1)  # n x 3
+    best = np.nanmin(np.where(np.isfinite(C), C, np.inf), 1)
+    # model choice among admissible layouts
+    preds = []
+    for L in LAYOUTS:
+        f = set_features(prof["lens"], prof["range"], prof["pairs"], np.full(n, L))
+        preds.append(model.predict(f)[:, 0])
+    P = np.stack(preds, 1)
+    P = np.where(np.isfinite(C), P, np.inf)
+    choice = np.argmin(P, 1)
+    chosen = C[np.arange(n), choice]
+    heur_col = np.where(prof["heuristic"] == BITSET, 1, 0)  # heuristic uses uint or bitset
+    heur_cost = C[np.arange(n), heur_col]
+    m = staged & np.isfinite(best) & np.isfinite(chosen) & np.isfinite(heur_cost)
+    total_best = best[m].sum()
+    finite = np.isfinite(C) & (C > 0)
+    err = np.abs(np.expm1(P[finite]) - C[finite]) / C[finite]
+    return {
+        "sets_staged": int(staged.sum()),
+        "median_abs_pct_error": float(np.median(err) * 100) if err.size else None,
+        "regret_learned_pct": float((chosen[m].sum() / total_best - 1) * 100) if total_best else None,
+        "regret_heuristic_pct": float((heur_cost[m].sum() / total_best - 1) * 100) if total_best else None,
+        "choice_hist": {"uint": int((choice[staged] == 0).sum()), "bitset": int((choice[staged] == 1).sum()),
+                        "block": int((choice[staged] == 2).sum())},
+    }
+
+
+def train_from_trie(E, trie, passes=2, epochs=60):
+    """Profile `trie`, train the cost model on the logs, evaluate it.
+    Returns (model, info)."""
+    prof = profile(E, trie, reps=passes)
+    x, y = dataset(prof)
+    model, losses = train(E, x, y, ctx=trie.ctx, epochs=epochs)
+    info = evaluate(E, model, prof)
+    info["train_rows"] = int(len(x))
+    info["final_loss"] = float(np.mean(losses[-20:])) if losses else None
+    return model, info

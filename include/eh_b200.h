@@ -1,0 +1,236 @@
+/* eh_b200.h -- C ABI of the B200 storage-engine hot path.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, no torch or C++ types.
+ * Every function returns eh_status (EH_OK == 0) and never aborts; the text
+ * of the last failure on the calling thread is returned by eh_last_error().
+ *
+ * Each entry point names the reference interface it replaces (paths are
+ * relative to the EmptyHeaded repository).  The reference is a C++ template
+ * library driven by generated query code; the drop-in mapping is written
+ * out in INTEGRATION.md.
+ */
+#ifndef EH_B200_H
+#define EH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int eh_status;
+enum {
+  EH_OK = 0,
+  EH_ERR_INVALID = 1,     /* bad argument */
+  EH_ERR_CUDA = 2,        /* CUDA runtime error */
+  EH_ERR_OOM = 3,         /* device allocation failed */
+  EH_ERR_TIMEOUT = 4,     /* a bounded device wait gave up */
+  EH_ERR_UNSUPPORTED = 5, /* request outside what the build supports */
+  EH_ERR_IO = 6,          /* file read/write failed */
+  EH_ERR_NO_DEVICE = 7    /* no CUDA device visible */
+};
+
+/* Set layouts; the codes are the reference's type::layout values
+ * (storage_engine/include/utils/common.hpp:83-91). */
+enum {
+  EH_LAYOUT_RANGE_BITSET = 0,
+  EH_LAYOUT_UINTEGER = 1,
+  EH_LAYOUT_BLOCK_BITSET = 3
+};
+
+/* How a trie picks each level-1 set's layout.
+ * HEURISTIC: the reference density rule, hybrid::get_type
+ *   (layouts/hybrid.hpp:103-111, utils/common.hpp:60-66).
+ * LEARNED: the cost model loaded with eh_trie_build (falls back to the
+ *   heuristic where the model abstains).
+ * FORCED: every set gets eh_layout_config.forced_layout. */
+enum { EH_POLICY_HEURISTIC = 0, EH_POLICY_LEARNED = 1, EH_POLICY_FORCED = 2 };
+
+/* Named generic-join plans executed as one device bag each. */
+enum {
+  EH_QUERY_TRIANGLE = 0, /* TriangleAgg(;z) :- Edge(a,b),Edge(b,c),Edge(a,c),z:long<-[COUNT(*)] */
+  EH_QUERY_CLIQUE4 = 1,  /* FliqueAgg(;z) :- 4-clique, COUNT(*) */
+  EH_QUERY_LOLLIPOP = 2, /* LollipopAgg(;z) :- triangle + Edge(a,x), COUNT(*) (2 bags) */
+  EH_QUERY_BARBELL = 3   /* BarbellAgg(;w) :- two triangles + Edge(a,x), COUNT(*) (2 bags) */
+};
+
+typedef struct eh_context eh_context;
+typedef struct eh_trie eh_trie;
+typedef struct eh_model eh_model;
+
+/* ------------------------------------------------------------- context */
+const char* eh_last_error(void);
+const char* eh_version(void);
+
+/* Replaces thread_pool::initializeThreadPool / deleteThreadPool
+ * (storage_engine/include/utils/thread_pool.hpp:16-41): owns the device,
+ * a stream and scratch memory. */
+eh_status eh_context_create(int device, eh_context** out);
+eh_status eh_context_destroy(eh_context* ctx);
+eh_status eh_context_sync(eh_context* ctx);
+/* the cudaStream_t the context launches on */
+eh_status eh_context_stream(eh_context* ctx, void** stream);
+
+/* Plain device memory for callers without a CUDA runtime of their own. */
+eh_status eh_device_alloc(eh_context* ctx, uint64_t bytes, void** out);
+eh_status eh_device_free(eh_context* ctx, void* p);
+eh_status eh_memcpy(eh_context* ctx, void* dst, const void* src, uint64_t bytes);
+
+/* ------------------------------------------------------- input pipeline
+ * Seeded edge-sample generators (device).  Outputs are device arrays of m
+ * raw samples (u[i], v[i]) allocated with eh_device_alloc. */
+eh_status eh_graph_er(eh_context* ctx, uint64_t seed, uint32_t n, uint64_t m, uint32_t** u, uint32_t** v);
+eh_status eh_graph_rmat(eh_context* ctx, uint64_t seed, int scale, uint64_t m, double a, double b, double c,
+                        uint32_t** u, uint32_t** v);
+eh_status eh_graph_chunglu(eh_context* ctx, uint64_t seed, uint32_t n, uint64_t m, double gamma, uint32_t** u,
+                           uint32_t** v);
+/* Symmetrise, drop self-loops, dedup, relabel nodes of degree > 0 by
+ * (degree, id) ascending, then keep src < dst (symmetric == 0) or both
+ * directions (symmetric == 1).  Output rows sorted by (src, dst), device
+ * arrays from eh_device_alloc.  Stands in for the reference's
+ * loadAndEncode step (codegen/create/createDB.scala:16-39), whose
+ * order-preserving dictionary encoding is the identity on these ids. */
+eh_status eh_graph_preprocess(eh_context* ctx, const uint32_t* u, const uint32_t* v, uint64_t m, int symmetric,
+                              uint32_t** src, uint32_t** dst, uint64_t* rows, uint32_t* nodes);
+
+/* ------------------------------------------------------------------ trie */
+typedef struct {
+  int policy;          /* EH_POLICY_* */
+  int forced_layout;   /* EH_LAYOUT_* when policy == EH_POLICY_FORCED */
+  const eh_model* model; /* EH_POLICY_LEARNED */
+  /* Per-set cap on range-bitset bytes (12 per word) for FORCED and LEARNED.
+   * Nonzero: a set over it, or over 16 words per element plus 64, keeps the
+   * heuristic layout.  0: no cap for FORCED; LEARNED always applies the
+   * per-element bound. */
+  uint64_t max_bitset_bytes;
+} eh_layout_config;
+
+typedef struct {
+  uint64_t rows;        /* distinct tuples */
+  uint32_t n_head;      /* distinct first-column values */
+  uint32_t n_nodes;     /* value domain: max value + 1 */
+  uint32_t head_layout; /* layout of the head set */
+  uint32_t n_uinteger, n_range_bitset, n_block_bitset; /* level-1 set layouts */
+  uint64_t bitset_words, block_count;
+  uint64_t device_bytes;
+  uint32_t max_set;     /* largest level-1 set */
+  float build_ms;       /* device time of the build */
+} eh_trie_info;
+
+/* Two-level trie from an encoded binary relation: rows (col0[i], col1[i]),
+ * any order, duplicates allowed.  Replaces the constructor
+ * Trie<A,M>::Trie(path, max_set_sizes, attr_in, annotations)
+ * (storage_engine/src/Trie.cpp:380-510) for two uint32 columns.
+ * cols_on_device != 0: col0/col1 are device pointers. */
+eh_status eh_trie_build(eh_context* ctx, const uint32_t* col0, const uint32_t* col1, uint64_t n_rows,
+                        int cols_on_device, const eh_layout_config* cfg, eh_trie** out);
+/* Re-pick level-1 set layouts of an existing trie (same elements). */
+eh_status eh_trie_relayout(eh_context* ctx, eh_trie* trie, const eh_layout_config* cfg);
+/* Replaces Trie<A,M>::~Trie (storage_engine/include/Trie.hpp:58-60). */
+eh_status eh_trie_free(eh_trie* trie);
+eh_status eh_trie_info_get(const eh_trie* trie, eh_trie_info* out);
+/* Host copy of the trie's sets, the content Trie::foreach walks
+ * (storage_engine/src/Trie.cpp:130-160): head[n_head], off[n_head+1],
+ * vals[rows], layout[n_head] (any pointer may be NULL). */
+eh_status eh_trie_export(const eh_trie* trie, uint32_t* head, uint64_t* off, uint32_t* vals, uint8_t* layout);
+/* Reference-format bytes of level-1 set i (Set<hybrid>::get_data and
+ * number_of_bytes, trie/set/Set.hpp:18-24): uinteger = u32[n];
+ * range_bitset = [u64 start word][u64 words][u32 rank]
+ * (layouts/range_bitset.hpp:123-157); block_bitset = per block
+ * [u32 block id][u32 start index][4 x u64] (layouts/block_bitset.hpp:112-131).
+ * set_index == UINT32_MAX selects the head set.  *nbytes receives the size;
+ * out may be NULL to query it. */
+eh_status eh_trie_set_bytes(const eh_trie* trie, uint32_t set_index, uint8_t* out, uint64_t cap, uint64_t* nbytes,
+                            uint8_t* layout);
+
+/* --------------------------------------------------------------- set ops
+ * Pairwise intersection of sets given as sorted uint32 runs in one packed
+ * host array: set k is elems[set_off[k] .. set_off[k+1]).  Each set is
+ * laid out on the device with layouts[k] (EH_LAYOUT_*), then pair p
+ * intersects sets pair_a[p] and pair_b[p] with the kernel for that layout
+ * pair.  Replaces ops::set_intersect (trie/set/ops/intersection/set.hpp:9-167):
+ * counts[p] is the aggregate result; when out_off != NULL the
+ * materialized elements of pair p are written to
+ * out_elems[out_off[p] .. out_off[p] + counts[p]) (out_off[p] must leave
+ * room for min(|A|,|B|) elements). */
+eh_status eh_set_intersect_batch(eh_context* ctx, const uint32_t* elems, const uint64_t* set_off, uint32_t n_sets,
+                                 const uint8_t* layouts, const uint32_t* pair_a, const uint32_t* pair_b,
+                                 uint32_t n_pairs, uint64_t* counts, const uint64_t* out_off, uint32_t* out_elems);
+
+/* ------------------------------------------------------------- queries */
+typedef struct {
+  int warps_per_block;   /* 0 = tuned default */
+  int chunk_pairs;       /* target (v,w) pairs per work item; 0 = tuned default */
+  int big_item_pairs;    /* items above this go to the CTA-wide bucket; 0 = default */
+  int smem_words;        /* per-warp shared staging capacity in u32 words; 0 = default */
+  int record_timings;    /* 1: log per-item device time for the cost model */
+  uint64_t spin_limit;   /* bound on device queue waits; 0 = default */
+  int shard_index;       /* run work items i with i % shard_count == shard_index */
+  int shard_count;       /* 0 or 1: all items (multi-GPU ranks split the plan) */
+} eh_exec_config;
+
+typedef struct {
+  float query_ms;        /* device time from first launch to result */
+  float kernel_ms;       /* device time of the intersection kernel(s) */
+  uint32_t launches;     /* kernels launched */
+  uint64_t work_items;
+  uint64_t wedges;       /* (v,w) pairs probed */
+  uint64_t algorithmic_bytes; /* 4*sum over edges (d+(u)+d+(v)) for triangle */
+  int timed_out;
+} eh_query_stats;
+
+/* Runs one named COUNT plan over `trie` (the Edge relation in ordering
+ * [0,1]) on the device and returns the aggregate.  Replaces the generated
+ * bag code run_<i> (query_compiler/.../codegen/query/EHGenerator.scala:728-838)
+ * with its ParTrieBuilder::build_aggregated_set / par_foreach_aggregate
+ * loop nest (storage_engine/include/TrieBuilder.hpp:117-165,
+ * storage_engine/src/TrieBuilder.cpp:451-578) and par::reducer
+ * (storage_engine/include/utils/parallel.hpp:8-34).  The result is the
+ * count modulo 2^64 (the reference's signed long, bit for bit). */
+eh_status eh_query_count(eh_context* ctx, const eh_trie* trie, int query, const eh_exec_config* cfg,
+                         uint64_t* result, eh_query_stats* stats);
+
+/* Same plan over many tries in one persistent launch; results[g] per
+ * trie. */
+eh_status eh_query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t n_tries, int query,
+                                 const eh_exec_config* cfg, uint64_t* results, eh_query_stats* stats);
+
+/* Per-head-entry triangle annotation T(a) (the annotated bag of
+ * lollipop/barbell, TrieBuilder::set_annotation, TrieBuilder.cpp:428-446),
+ * copied to host annot[n_head]. */
+eh_status eh_triangle_annotation(eh_context* ctx, const eh_trie* trie, const eh_exec_config* cfg, uint64_t* annot);
+
+/* Host-buffer convenience: copy a CSR trie (head, off, vals) from host
+ * memory, lay it out with cfg, count, and return; the reference-facing
+ * call with host inputs. */
+eh_status eh_query_count_host_csr(eh_context* ctx, const uint32_t* head, uint32_t n_head, const uint64_t* off,
+                                  const uint32_t* vals, uint32_t n_nodes, const eh_layout_config* cfg, int query,
+                                  const eh_exec_config* ecfg, uint64_t* result, eh_query_stats* stats);
+
+/* Records of per-item intersection timings from the last query run with
+ * record_timings, for the cost model.  One record per work item, 8 floats:
+ * [|N(b)|, pairs probed, density of N(b), range of N(b), layout of N(b),
+ * probe mode, b (uint32 bit pattern), SM cycles].  rec must hold cap
+ * records; *n receives the count. */
+eh_status eh_timing_records(eh_context* ctx, float* rec, uint64_t cap, uint64_t* n);
+
+/* --------------------------------------------------------- cost model
+ * A small fp32 MLP trained on the device by hand-written kernels.  dims:
+ * layer widths d0..dL.  Parameters packed (W0,b0,W1,b1,...) with W row-major
+ * [d_{l+1} x d_l]. */
+eh_status eh_model_create(eh_context* ctx, int n_layers, const int* dims, uint64_t seed, eh_model** out);
+eh_status eh_model_free(eh_model* m);
+eh_status eh_model_params(eh_model* m, float* host_params, uint64_t cap, uint64_t* n, int set);
+/* one SGD step on a batch (host arrays x[batch*d0], y[batch*dL]); returns the loss */
+eh_status eh_model_train(eh_context* ctx, eh_model* m, const float* x, const float* y, uint32_t batch, float lr,
+                         uint32_t steps, float* loss);
+/* loss and gradient without updating (host arrays); grad has n_params entries */
+eh_status eh_model_loss_grad(eh_context* ctx, eh_model* m, const float* x, const float* y, uint32_t batch,
+                             float* loss, float* grad);
+eh_status eh_model_predict(eh_context* ctx, eh_model* m, const float* x, uint32_t batch, float* y);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EH_B200_H */

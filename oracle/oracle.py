@@ -191,6 +191,25 @@ def range_bitset(a):
     return out[:nb]
 
 
+def block_bitset(a):
+    """block_bitset::build (layouts/block_bitset.hpp:112-131): per non-empty
+    256-value block, [u32 block id][u32 index of its first element][4 x u64]."""
+    a = np.ascontiguousarray(a, np.uint32)
+    out = bytearray()
+    i = 0
+    while i < len(a):
+        bid = int(a[i]) >> 8
+        j = i
+        words = [0, 0, 0, 0]
+        while j < len(a) and (int(a[j]) >> 8) == bid:
+            x = int(a[j]) & 255
+            words[x >> 6] |= 1 << (x & 63)
+            j += 1
+        out += np.array([bid, i], np.uint32).tobytes() + np.array(words, np.uint64).tobytes()
+        i = j
+    return np.frombuffer(bytes(out), np.uint8)
+
+
 def intersect(a, b):
     a = np.ascontiguousarray(a, np.uint32)
     b = np.ascontiguousarray(b, np.uint32)
