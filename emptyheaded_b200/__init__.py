@@ -15,13 +15,17 @@ reference's storage-engine API:
 It never computes on the host: if the shared library or a GPU is missing,
 calls raise.
 """
+import atexit
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libeh_b200.so")
+# EH_B200_LIB selects another build of the same library (a variant built
+# with emptyheaded_b200.build.build(libdir=...)); default: the in-tree one
+LIB_PATH = os.environ.get("EH_B200_LIB") or os.path.join(_HERE, "_lib", "libeh_b200.so")
 
 # status codes and enums (include/eh_b200.h)
 EH_OK = 0
@@ -51,7 +55,7 @@ class TrieInfo(ctypes.Structure):
 
 
 class ExecConfig(ctypes.Structure):
-    _fields_ = [("warps_per_block", ctypes.c_int), ("chunk_pairs", ctypes.c_int), ("big_item_pairs", ctypes.c_int),
+    _fields_ = [("warps_per_block", ctypes.c_int), ("chunk_pairs", ctypes.c_int), ("long_row", ctypes.c_int),
                 ("smem_words", ctypes.c_int), ("record_timings", ctypes.c_int), ("spin_limit", ctypes.c_uint64),
                 ("shard_index", ctypes.c_int), ("shard_count", ctypes.c_int)]
 
@@ -136,17 +140,29 @@ def _ptr(a):
 
 
 # ------------------------------------------------------------------ context
+_live_contexts = weakref.WeakSet()
+
+
 class Context:
     """Device, stream and events (the role of the reference's thread pool,
-    utils/thread_pool.hpp:16-41)."""
+    utils/thread_pool.hpp:16-41).  Tries, models and device arrays made in a
+    context must be freed before it; close() frees whatever is still alive,
+    and every open context is closed at interpreter exit in that order."""
 
     def __init__(self, device=0):
         h = ctypes.c_void_p()
         _check(lib().eh_context_create(device, ctypes.byref(h)))
         self.h = h
+        self._children = weakref.WeakSet()
+        _live_contexts.add(self)
+
+    def _adopt(self, obj):
+        self._children.add(obj)
 
     def close(self):
-        if self.h:
+        if getattr(self, "h", None):
+            for c in list(self._children):
+                c.free()
             lib().eh_context_destroy(self.h)
             self.h = None
 
@@ -165,6 +181,15 @@ class Context:
         return s.value
 
 
+@atexit.register
+def _close_all():
+    for c in list(_live_contexts):
+        try:
+            c.close()
+        except Exception:
+            pass
+
+
 _default = None
 
 
@@ -180,6 +205,7 @@ class DeviceArray:
 
     def __init__(self, ctx, ptr, n):
         self.ctx, self.ptr, self.n = ctx, ptr, n
+        ctx._adopt(self)
 
     def free(self):
         if self.ptr:
@@ -240,11 +266,11 @@ def _layout_cfg(policy=HEURISTIC, forced=UINTEGER, model=None, max_bitset_bytes=
     return c
 
 
-def _exec_cfg(warps=0, chunk=0, smem_words=0, record=False, shard=(0, 1)):
+def _exec_cfg(warps=0, chunk=0, smem_words=0, record=False, shard=(0, 1), long_row=0):
     e = ExecConfig()
     e.warps_per_block = warps
     e.chunk_pairs = chunk
-    e.big_item_pairs = 0
+    e.long_row = long_row
     e.smem_words = smem_words
     e.record_timings = 1 if record else 0
     e.spin_limit = 0
@@ -277,6 +303,7 @@ class Trie:
             _check(lib().eh_trie_build(self.ctx.h, _ptr(c0), _ptr(c1), len(c0), 0, ctypes.byref(cfg),
                                        ctypes.byref(h)))
         self.h = h
+        self.ctx._adopt(self)
 
     def free(self):
         if getattr(self, "h", None):
@@ -319,11 +346,18 @@ class Trie:
         _check(lib().eh_trie_set_bytes(self.h, idx, _ptr(out), n.value, ctypes.byref(n), ctypes.byref(lay)))
         return out[: n.value], lay.value
 
-    def count(self, query="triangle", warps=0, chunk=0, smem_words=0, record=False, stats=False, shard=(0, 1)):
+    def count(self, query="triangle", warps=0, chunk=0, smem_words=0, record=False, stats=False, shard=(0, 1),
+              long_row=0, config=None):
         """Run a named COUNT plan; returns the count (and stats if asked).
         shard=(i, n) runs the i-th of n round-robin shares of the work items
-        (the partial counts of the n shares sum to the count)."""
-        e = _exec_cfg(warps, chunk, smem_words, record, shard)
+        (the partial counts of the n shares sum to the count).  `config`
+        (a dict from emptyheaded_b200.autotune) supplies the schedule knobs."""
+        if config:
+            warps = config.get("warps", warps)
+            chunk = config.get("chunk", chunk)
+            smem_words = config.get("smem_words", smem_words)
+            long_row = config.get("long_row", long_row)
+        e = _exec_cfg(warps, chunk, smem_words, record, shard, long_row)
         r = ctypes.c_uint64()
         st = QueryStats()
         _check(lib().eh_query_count(self.ctx.h, self.h, QUERIES[query], ctypes.byref(e), ctypes.byref(r),
@@ -353,11 +387,13 @@ def count_batched(tries, query="triangle", chunk=0, stats=False):
     return res
 
 
-def count_host_csr(head, off, vals, n_nodes, query="triangle", policy=HEURISTIC, model=None, ctx=None, stats=False):
+def count_host_csr(head, off, vals, n_nodes, query="triangle", policy=HEURISTIC, model=None, ctx=None, stats=False,
+                   config=None):
     """Host CSR in, count out: the reference-facing call with host buffers."""
     ctx = ctx or default_context()
     cfg = _layout_cfg(policy, UINTEGER, model)
-    e = _exec_cfg()
+    c = config or {}
+    e = _exec_cfg(c.get("warps", 0), c.get("chunk", 0), c.get("smem_words", 0), long_row=c.get("long_row", 0))
     r = ctypes.c_uint64()
     st = QueryStats()
     _check(lib().eh_query_count_host_csr(ctx.h, _ptr(head), len(head), _ptr(off), _ptr(vals), n_nodes,
@@ -423,6 +459,7 @@ class Model:
         h = ctypes.c_void_p()
         _check(lib().eh_model_create(self.ctx.h, len(dims) - 1, d, seed, ctypes.byref(h)))
         self.h = h
+        self.ctx._adopt(self)
 
     def free(self):
         if getattr(self, "h", None):

@@ -45,14 +45,18 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose=False, extra_flags=()):
-    os.makedirs(OBJDIR, exist_ok=True)
+def build(verbose=False, extra_flags=(), libdir=None):
+    """Compile and link; `libdir` (default _lib) and `extra_flags` let a
+    variant build land elsewhere without touching the in-tree library."""
+    objdir = OBJDIR if libdir is None else os.path.join(libdir, "obj")
+    lib = LIB if libdir is None else os.path.join(libdir, "libeh_b200.so")
+    os.makedirs(objdir, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     hdrs = _headers()
     jobs = []
     objs = []
     for s in srcs:
-        o = os.path.join(OBJDIR, os.path.basename(s)[:-3] + ".o")
+        o = os.path.join(objdir, os.path.basename(s)[:-3] + ".o")
         objs.append(o)
         if _stale(o, [s] + hdrs):
             jobs.append([nvcc()] + ARCH + NVCC_FLAGS + list(extra_flags) + ["-c", s, "-o", o])
@@ -66,9 +70,9 @@ def build(verbose=False, extra_flags=()):
 
     with cf.ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:
         list(ex.map(run, jobs))
-    if jobs or _stale(LIB, objs):
-        run([nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
-    return LIB
+    if jobs or _stale(lib, objs):
+        run([nvcc()] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart"])
+    return lib
 
 
 if __name__ == "__main__":

@@ -20,9 +20,25 @@
 
 namespace eh {
 
-constexpr int kDefaultWarps = 8;
-constexpr int kDefaultSmemWords = 2048;  // per warp: 8 KB
-constexpr int kDefaultChunk = 8192;
+// Register budget of the intersection kernels, set by their launch bounds
+// (threads per block, optional blocks per SM); the block size knob is
+// capped to match.
+#ifndef EH_TRI_MAX_THREADS
+#define EH_TRI_MAX_THREADS 512
+#endif
+#ifdef EH_TRI_MIN_BLOCKS
+#define EH_TRI_LAUNCH_BOUNDS __launch_bounds__(EH_TRI_MAX_THREADS, EH_TRI_MIN_BLOCKS)
+#else
+#define EH_TRI_LAUNCH_BOUNDS __launch_bounds__(EH_TRI_MAX_THREADS)
+#endif
+constexpr int kMaxWarps = EH_TRI_MAX_THREADS / 32;  // per block
+constexpr int kDefaultWarps = kMaxWarps < 8 ? kMaxWarps : 8;
+constexpr uint32_t kDefaultLongRow = 32;  // rows with at least this many candidates run warp-wide
+// Defaults measured on B200 at R-MAT-22 (4 KB of staging per warp leaves
+// room for 32 resident warps; 32K-probe items amortise staging); the
+// autotuner (emptyheaded_b200/autotune.py) re-picks them per trie.
+constexpr int kDefaultSmemWords = 1024;  // per warp
+constexpr int kDefaultChunk = 32768;
 
 struct RevView {
   const uint64_t* rev_off;
@@ -42,6 +58,7 @@ struct ExecParams {
   int smem_words;
   uint32_t chunk;
   uint32_t shard_index, shard_count;
+  uint32_t long_row;
 };
 
 static ExecParams exec_params(const eh_exec_config* cfg) {
@@ -49,10 +66,11 @@ static ExecParams exec_params(const eh_exec_config* cfg) {
   p.warps = (cfg && cfg->warps_per_block > 0) ? cfg->warps_per_block : kDefaultWarps;
   p.smem_words = (cfg && cfg->smem_words > 0) ? cfg->smem_words : kDefaultSmemWords;
   p.chunk = (cfg && cfg->chunk_pairs > 0) ? (uint32_t)cfg->chunk_pairs : (uint32_t)kDefaultChunk;
+  p.long_row = (cfg && cfg->long_row > 0) ? (uint32_t)cfg->long_row : kDefaultLongRow;
   p.shard_count = (cfg && cfg->shard_count > 1) ? (uint32_t)cfg->shard_count : 1u;
   p.shard_index = (cfg && cfg->shard_count > 1) ? (uint32_t)cfg->shard_index : 0u;
   EH_REQUIRE(p.shard_index < p.shard_count, EH_ERR_INVALID, "shard_index must be below shard_count");
-  p.warps = std::max(1, std::min(p.warps, 32));
+  p.warps = std::max(1, std::min(p.warps, kMaxWarps));
   p.smem_words = std::max(64, std::min(p.smem_words, 16384)) & ~1;
   return p;
 }
@@ -172,9 +190,42 @@ __device__ __forceinline__ uint32_t probe(const Staged& s, uint32_t w) {
 // flattening (row, element) pairs over the 32 lanes.  kAnnot adds each
 // hit to the annotation of the row's source (and, for symmetric tries,
 // of the matched element).
+// owner lane of flattened pair q: the number of lanes whose inclusive
+// prefix is <= q (q < total guarantees a result below 32)
+__device__ __forceinline__ uint32_t owner_lane(uint32_t incl, uint32_t q) {
+  uint32_t j = 0;
+#pragma unroll
+  for (int step = 16; step; step >>= 1) {
+    const uint32_t tj = __shfl_sync(kFull, incl, j + step - 1);
+    if (tj <= q) j += step;
+  }
+  return j;
+}
+
+template <bool kAnnot>
+__device__ __forceinline__ void annotate_hit(const TrieView& t, const RevView& r, unsigned long long* annot,
+                                             uint32_t src, uint32_t w) {
+  if (r.dir == DIR_SYM) {
+    atomicAdd(annot + src, 2ull);
+    atomicAdd(annot + __ldg(t.head_index + w), 2ull);
+  } else {
+    atomicAdd(annot + src, 1ull);
+  }
+}
+
+// Rows whose source set N(a) is also a range bitset, against a bitset N(b),
+// are intersected word by word (64-bit AND + popcount over the overlap of
+// the candidate value range [v0, v1] with both word ranges) whenever that
+// takes fewer words than the row has candidate elements; the reference's
+// bitset ∩ bitset path (ops/intersection/bitset.hpp:526-567, 619-661).
+// Word rows run warp-cooperatively one row at a time (coalesced 8-byte
+// loads of N(a)'s words); the other rows are flattened (row, element)
+// pairs over the lanes, two pairs per lane per trip for memory-level
+// parallelism.
 template <int P, bool kAnnot>
 __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView& t, const RevView& r, uint32_t kb,
-                                                uint32_t ke, unsigned long long* annot) {
+                                                uint32_t ke, uint32_t long_row, unsigned long long* annot) {
+  constexpr bool kBits = (P == P_SBITS || P == P_GBITS);
   const uint32_t lane = lane_id();
   uint64_t cnt = 0;
   for (uint32_t k0 = kb; k0 < ke; k0 += 32) {
@@ -183,35 +234,105 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
     if (k < ke) {
       lo = __ldg(r.rev_lo + k);
       len = __ldg(r.rev_hi + k) - lo;
-      if (kAnnot) src = __ldg(r.rev_src + k);
+      if (kAnnot || kBits) src = __ldg(r.rev_src + k);
     }
+    // ---- word rows
+    if (kBits) {
+      bool word_row = false;
+      uint32_t v0 = 0, v1 = 0, wlo = 0, whi = 0;
+      uint64_t abase = 0;
+      if (len && __ldg(t.layout + src) == EH_LAYOUT_RANGE_BITSET) {
+        v0 = __ldg(t.vals + lo);
+        v1 = __ldg(t.vals + lo + len - 1);
+        const SetAux aa = t.aux[src];
+        const uint32_t lo_w = max(max(v0 >> 6, aa.start), st.start);
+        const uint32_t hi_w = min(min(v1 >> 6, aa.start + aa.n - 1), st.start + st.n - 1);
+        const uint32_t words = hi_w >= lo_w ? hi_w - lo_w + 1 : 0;
+        if (words < len) {
+          word_row = true;
+          wlo = lo_w;
+          whi = hi_w;
+          abase = aa.off - aa.start;  // word w of N(a) is bs_words[abase + w]
+        }
+      }
+      uint32_t rows = __ballot_sync(kFull, word_row && whi >= wlo);
+      if (word_row) len = 0;  // handled here, not in the element loop
+      while (rows) {
+        const int j = __ffs(rows) - 1;
+        rows &= rows - 1;
+        const uint32_t a_lo = __shfl_sync(kFull, wlo, j), a_hi = __shfl_sync(kFull, whi, j);
+        const uint32_t b0 = __shfl_sync(kFull, v0, j), b1 = __shfl_sync(kFull, v1, j);
+        const uint64_t base = __shfl_sync(kFull, abase, j);
+        const uint32_t src_j = __shfl_sync(kFull, src, j);
+        uint32_t c = 0;
+        for (uint32_t w = a_lo + lane; w <= a_hi; w += 32) {
+          uint64_t m = ~0ull;
+          if (w == (b0 >> 6)) m &= ~0ull << (b0 & 63);
+          if (w == (b1 >> 6)) m &= ~0ull >> (63 - (b1 & 63));
+          const uint64_t bw = (P == P_SBITS) ? st.words[w - st.start] : __ldg(st.words + (w - st.start));
+          uint64_t x = __ldg(t.bs_words + base + w) & bw & m;
+          c += __popcll(x);
+          if (kAnnot) {
+            while (x) {
+              const uint32_t bit = __ffsll((long long)x) - 1;
+              annotate_hit<kAnnot>(t, r, annot, src_j, (w << 6) | bit);
+              x &= x - 1;
+            }
+          }
+        }
+        cnt += c;
+      }
+    }
+    // ---- long element rows: one row at a time across the warp, two
+    // coalesced elements per lane per trip, no owner search
+    {
+      const bool is_long = len >= long_row;
+      uint32_t rows = __ballot_sync(kFull, is_long);
+      const uint32_t rlen = len;
+      if (is_long) len = 0;
+      while (rows) {
+        const int j = __ffs(rows) - 1;
+        rows &= rows - 1;
+        const uint32_t rlo = __shfl_sync(kFull, lo, j), rn = __shfl_sync(kFull, rlen, j);
+        uint32_t src_j = 0;
+        if (kAnnot) src_j = __shfl_sync(kFull, src, j);
+        const uint32_t* row = t.vals + rlo;
+        for (uint32_t i = lane; i < rn; i += 64) {
+          const bool second = i + 32 < rn;
+          const uint32_t w0 = __ldg(row + i);
+          const uint32_t w1 = second ? __ldg(row + i + 32) : 0;
+          const uint32_t h0 = probe<P>(st, w0);
+          const uint32_t h1 = second ? probe<P>(st, w1) : 0u;
+          cnt += h0 + h1;
+          if (kAnnot) {
+            if (h0) annotate_hit<kAnnot>(t, r, annot, src_j, w0);
+            if (h1) annotate_hit<kAnnot>(t, r, annot, src_j, w1);
+          }
+        }
+      }
+    }
+    // ---- short element rows, flattened
     const uint32_t incl = warp_incl_scan(len);
     const uint32_t total = __shfl_sync(kFull, incl, 31);
     const uint32_t excl = incl - len;
-    for (uint32_t p = 0; p < total; p += 32) {
-      const uint32_t q = p + lane;
-      uint32_t j = 0;
-#pragma unroll
-      for (int step = 16; step; step >>= 1) {
-        const uint32_t tj = __shfl_sync(kFull, incl, j + step - 1);
-        if (tj <= q) j += step;
+    for (uint32_t p = 0; p < total; p += 64) {
+      const uint32_t q0 = p + lane, q1 = p + 32 + lane;
+      const uint32_t j0 = owner_lane(incl, q0), j1 = owner_lane(incl, q1);
+      const uint32_t lo0 = __shfl_sync(kFull, lo, j0), ex0 = __shfl_sync(kFull, excl, j0);
+      const uint32_t lo1 = __shfl_sync(kFull, lo, j1), ex1 = __shfl_sync(kFull, excl, j1);
+      uint32_t s0 = 0, s1 = 0;
+      if (kAnnot) {
+        s0 = __shfl_sync(kFull, src, j0);
+        s1 = __shfl_sync(kFull, src, j1);
       }
-      const uint32_t lo_j = __shfl_sync(kFull, lo, j);
-      const uint32_t ex_j = __shfl_sync(kFull, excl, j);
-      uint32_t src_j = 0;
-      if (kAnnot) src_j = __shfl_sync(kFull, src, j);
-      if (q < total) {
-        const uint32_t w = __ldg(t.vals + lo_j + (q - ex_j));
-        const uint32_t hit = probe<P>(st, w);
-        cnt += hit;
-        if (kAnnot && hit) {
-          if (r.dir == DIR_SYM) {
-            atomicAdd(annot + src_j, 2ull);
-            atomicAdd(annot + __ldg(t.head_index + w), 2ull);
-          } else {
-            atomicAdd(annot + src_j, 1ull);
-          }
-        }
+      const uint32_t w0 = q0 < total ? __ldg(t.vals + lo0 + (q0 - ex0)) : 0;
+      const uint32_t w1 = q1 < total ? __ldg(t.vals + lo1 + (q1 - ex1)) : 0;
+      const uint32_t h0 = q0 < total ? probe<P>(st, w0) : 0u;
+      const uint32_t h1 = q1 < total ? probe<P>(st, w1) : 0u;
+      cnt += h0 + h1;
+      if (kAnnot) {
+        if (h0) annotate_hit<kAnnot>(t, r, annot, s0, w0);
+        if (h1) annotate_hit<kAnnot>(t, r, annot, s1, w1);
       }
     }
   }
@@ -258,6 +379,7 @@ __device__ __forceinline__ int stage_set(const TrieView& t, uint32_t hb, uint32_
 
 struct QueryOut {
   uint32_t shard_index, shard_count;  // this launch runs items shard_index + q * shard_count
+  uint32_t long_row;                  // size-class boundary of rows (warp-wide vs flattened)
   unsigned long long* total;   // per graph results (one per trie)
   unsigned long long* annot;   // per head entry annotation or null
   float* records;              // per item timing records or null
@@ -266,7 +388,7 @@ struct QueryOut {
 };
 
 template <bool kAnnot>
-__global__ void __launch_bounds__(1024) triangle_kernel(const TrieView* __restrict__ views,
+__global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict__ views,
                                                         const RevView* __restrict__ revs,
                                                         const Item* __restrict__ items, uint32_t n_items,
                                                         int cap_words, QueryOut out) {
@@ -298,11 +420,11 @@ __global__ void __launch_bounds__(1024) triangle_kernel(const TrieView* __restri
     unsigned long long* annot = kAnnot ? out.annot : nullptr;
     uint64_t c;
     switch (mode) {
-      case P_SBITS: c = stream_rows<P_SBITS, kAnnot>(st, t, r, item.kb, item.ke, annot); break;
-      case P_GBITS: c = stream_rows<P_GBITS, kAnnot>(st, t, r, item.kb, item.ke, annot); break;
-      case P_SLIST: c = stream_rows<P_SLIST, kAnnot>(st, t, r, item.kb, item.ke, annot); break;
-      case P_GLIST: c = stream_rows<P_GLIST, kAnnot>(st, t, r, item.kb, item.ke, annot); break;
-      default: c = stream_rows<P_GBLOCK, kAnnot>(st, t, r, item.kb, item.ke, annot); break;
+      case P_SBITS: c = stream_rows<P_SBITS, kAnnot>(st, t, r, item.kb, item.ke, out.long_row, annot); break;
+      case P_GBITS: c = stream_rows<P_GBITS, kAnnot>(st, t, r, item.kb, item.ke, out.long_row, annot); break;
+      case P_SLIST: c = stream_rows<P_SLIST, kAnnot>(st, t, r, item.kb, item.ke, out.long_row, annot); break;
+      case P_GLIST: c = stream_rows<P_GLIST, kAnnot>(st, t, r, item.kb, item.ke, out.long_row, annot); break;
+      default: c = stream_rows<P_GBLOCK, kAnnot>(st, t, r, item.kb, item.ke, out.long_row, annot); break;
     }
     c = warp_sum(c);
     if (kAnnot && r.dir == DIR_SYM && lane == 0 && c) atomicAdd(out.annot + item.hb, 2ull * c);
@@ -393,7 +515,7 @@ __device__ uint64_t clique_rows(const Staged& st, const TrieView& t, const RevVi
   return cnt;
 }
 
-__global__ void __launch_bounds__(1024) clique4_kernel(const TrieView* __restrict__ views,
+__global__ void EH_TRI_LAUNCH_BOUNDS clique4_kernel(const TrieView* __restrict__ views,
                                                        const RevView* __restrict__ revs,
                                                        const Item* __restrict__ items, uint32_t n_items,
                                                        int cap_words, QueryOut out) {
@@ -487,7 +609,7 @@ struct Launch {
 
 // Runs the intersection kernel of `query` over the concatenated plans of
 // n graphs; results accumulate into d_total[g].
-static Launch run_plans(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query, const ExecParams& ep,
+static Launch run_plans(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query, ExecParams ep,
                         bool annot, unsigned long long* d_total, unsigned long long* d_annot, float* d_records,
                         uint32_t* n_items_out, uint64_t* pairs_out) {
   cudaStream_t s = ctx->stream;
@@ -528,9 +650,21 @@ static Launch run_plans(eh_context* ctx, const eh_trie* const* tries, uint32_t n
   EH_CUDA(cudaMemcpyAsync(dv.p, hv.data(), n * sizeof(TrieView), cudaMemcpyHostToDevice, s));
   EH_CUDA(cudaMemcpyAsync(dr.p, hr.data(), n * sizeof(RevView), cudaMemcpyHostToDevice, s));
   EH_CUDA(cudaMemsetAsync(q.p, 0, 8, s));
-  QueryOut out{ep.shard_index, ep.shard_count, d_total, d_annot, d_records, q.p, q.p + 1};
+  QueryOut out{ep.shard_index, ep.shard_count, ep.long_row, d_total, d_annot, d_records, q.p, q.p + 1};
   const int threads = 32 * ep.warps;
-  const size_t smem = (size_t)ep.smem_words * 4 * ep.warps;
+  size_t smem = (size_t)ep.smem_words * 4 * ep.warps;
+  {
+    int dev = 0, optin = 0;
+    EH_CUDA(cudaGetDevice(&dev));
+    EH_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (smem > (size_t)optin) {
+      // shrink the per-warp region to what a block may hold (a staged set
+      // that no longer fits is probed in global memory instead)
+      EH_REQUIRE(query != EH_QUERY_CLIQUE4, EH_ERR_UNSUPPORTED, "4-clique staging exceeds shared memory");
+      ep.smem_words = (int)((optin / 4 / ep.warps) & ~1);
+      smem = (size_t)ep.smem_words * 4 * ep.warps;
+    }
+  }
   const void* kfn;
   if (query == EH_QUERY_CLIQUE4) {
     set_smem_attr(clique4_kernel, smem);

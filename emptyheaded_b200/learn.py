@@ -86,24 +86,50 @@ def dataset(prof):
     return np.concatenate(xs), np.concatenate(ys)
 
 
-def train(E, x, y, ctx=None, epochs=60, batch=4096, lr=0.02, seed=0):
-    """SGD on the device (eh_model_train) over shuffled minibatches."""
+def _fold(params, dims, mu_x, sd_x, mu_y, sd_y):
+    """Fold input standardisation into layer 0 and output scaling into the
+    last layer, so the device chooser evaluates the model on raw features."""
+    p = params.astype(np.float64).copy()
+    d0, d1 = dims[0], dims[1]
+    W0 = p[: d1 * d0].reshape(d1, d0)
+    b0 = p[d1 * d0: d1 * d0 + d1]
+    b0 -= W0 @ (mu_x / sd_x)
+    W0 /= sd_x[None, :]
+    o = 0
+    for l in range(len(dims) - 1):
+        o += dims[l + 1] * dims[l] + dims[l + 1]
+    dl, dp = dims[-1], dims[-2]
+    WL = p[o - dl - dl * dp: o - dl].reshape(dl, dp)
+    bL = p[o - dl: o]
+    WL *= sd_y
+    bL *= sd_y
+    bL += mu_y
+    return p.astype(np.float32)
+
+
+def train(E, x, y, ctx=None, epochs=40, batch=2048, lr=0.05, seed=0):
+    """SGD on the device (eh_model_train) over shuffled minibatches of
+    standardised features and targets; returns the model with the
+    standardisation folded into its weights."""
     model = E.Model(DIMS, seed=seed, ctx=ctx)
-    mu = float(y.mean())
-    # start the output bias at the mean target so SGD fits the residual
-    p = model.params()
-    p[-1] = mu
-    model.set_params(p)
+    mu_x = x.mean(0).astype(np.float64)
+    sd_x = x.std(0).astype(np.float64)
+    sd_x[sd_x < 1e-6] = 1.0
+    mu_y, sd_y = float(y.mean()), float(y.std()) or 1.0
+    xn = ((x - mu_x) / sd_x).astype(np.float32)
+    yn = ((y - mu_y) / sd_y).astype(np.float32)
     rng = np.random.default_rng(seed)
     n = len(x)
     losses = []
     for ep in range(epochs):
         perm = rng.permutation(n)
+        step_lr = lr * (0.1 if ep >= int(0.75 * epochs) else 1.0)
         for i in range(0, n, batch):
             idx = perm[i:i + batch]
             if len(idx) < 16:
                 continue
-            losses.append(model.train(x[idx], y[idx], lr=lr, steps=1))
+            losses.append(model.train(xn[idx], yn[idx], lr=step_lr, steps=1))
+    model.set_params(_fold(model.params(), DIMS, mu_x, sd_x, mu_y, sd_y))
     return model, losses
 
 

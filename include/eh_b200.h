@@ -162,7 +162,9 @@ eh_status eh_set_intersect_batch(eh_context* ctx, const uint32_t* elems, const u
 typedef struct {
   int warps_per_block;   /* 0 = tuned default */
   int chunk_pairs;       /* target (v,w) pairs per work item; 0 = tuned default */
-  int big_item_pairs;    /* items above this go to the CTA-wide bucket; 0 = default */
+  int long_row;          /* size-class boundary: rows with at least this many
+                            candidates run warp-wide, shorter ones are
+                            flattened over the lanes; 0 = default (32) */
   int smem_words;        /* per-warp shared staging capacity in u32 words; 0 = default */
   int record_timings;    /* 1: log per-item device time for the cost model */
   uint64_t spin_limit;   /* bound on device queue waits; 0 = default */

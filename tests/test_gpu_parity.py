@@ -206,6 +206,12 @@ def test_schedule_knobs_do_not_change_counts(eh, oracle):
         for chunk in (1, 64, 4096, 1 << 22):
             for smem in (64, 2048, 8192):
                 assert t.count("triangle", warps=warps, chunk=chunk, smem_words=smem) == want
+    for long_row in (1, 7, 32, 1 << 20):
+        assert t.count("triangle", long_row=long_row) == want
+    t.relayout(policy=2, forced=0, max_bitset_bytes=1 << 50)
+    for long_row in (1, 32, 1 << 20):
+        for smem in (64, 1024):
+            assert t.count("triangle", long_row=long_row, smem_words=smem) == want
 
 
 def test_batched_counts(eh, oracle):
@@ -227,3 +233,28 @@ def test_host_csr_entry(eh, oracle, golden):
     o = oracle.Trie(s, d)
     r = eh.count_host_csr(o.head, o.off, o.vals, nn)
     assert r == golden["synthetic"]["rmat_s12_ef16_s3"]["triangle"]
+
+
+def test_autotune_keeps_counts(eh, oracle):
+    from emptyheaded_b200 import autotune
+    u, v = oracle.gen_rmat(42, 16, 16 << 16)
+    s, d, _ = oracle.preprocess(u, v)
+    t = eh.Trie(s, d)
+    grid = {"smem_words": (512, 1024), "chunk": (4096, 32768), "long_row": (16, 64), "warps": (4, 8)}
+    best, log = autotune.tune(t, reps=1, rounds=1, grid=grid)
+    assert set(best) == set(autotune.DEFAULT) and len(log) >= 5
+    assert t.count("triangle", config=best) == 15754143
+
+
+def test_context_close_frees_dependents(eh, facebook):
+    """Closing a context first frees the tries and models made in it, so
+    no handle outlives its context (interpreter exit relies on this)."""
+    c = eh.Context(0)
+    p = facebook["pruned"]
+    t = eh.Trie(p[:, 0], p[:, 1], ctx=c)
+    m = eh.Model([6, 8, 1], ctx=c)
+    assert t.count("triangle") == 1612010
+    c.close()
+    assert t.h is None and m.h is None
+    t.free()
+    c.close()
