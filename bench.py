@@ -230,6 +230,9 @@ def ours_arm(args):
         torch.cuda.synchronize()
         qms, kms, launches = [], [], 0
         wall0 = time.time()
+        # NVTX range "timed": profiler captures select the timed steps with
+        # --nvtx --nvtx-include "timed/"
+        torch.cuda.nvtx.range_push("timed")
         for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -239,6 +242,7 @@ def ours_arm(args):
             kms.append(st["kernel_ms"])
             launches += st["launches"]
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         if world > 1:
             torch.distributed.barrier()
         wall = time.time() - wall0

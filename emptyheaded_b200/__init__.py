@@ -110,6 +110,10 @@ def lib():
             "eh_query_count_batched": [_P, _P, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ExecConfig), _P,
                                        ctypes.POINTER(QueryStats)],
             "eh_triangle_annotation": [_P, _P, ctypes.POINTER(ExecConfig), _P],
+            "eh_batch_create": [_P, _P, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ExecConfig),
+                                ctypes.POINTER(_P)],
+            "eh_batch_run": [_P, _P, _P, ctypes.POINTER(QueryStats)],
+            "eh_batch_free": [_P],
             "eh_query_count_host_csr": [_P, _P, ctypes.c_uint32, _P, _P, ctypes.c_uint32,
                                         ctypes.POINTER(LayoutConfig), ctypes.c_int, ctypes.POINTER(ExecConfig), _u64p,
                                         ctypes.POINTER(QueryStats)],
@@ -385,6 +389,41 @@ def count_batched(tries, query="triangle", chunk=0, stats=False):
     if stats:
         return res, {k: getattr(st, k) for k, _ in QueryStats._fields_}
     return res
+
+
+class Batch:
+    """Many tries, one plan, one CUDA-graph launch per run (eh_batch_*).
+    The tries must stay alive and keep their layouts while the batch lives."""
+
+    def __init__(self, tries, query="triangle", config=None):
+        self.ctx = tries[0].ctx
+        self.tries = list(tries)  # keep them alive
+        c = config or {}
+        e = _exec_cfg(c.get("warps", 0), c.get("chunk", 0), c.get("smem_words", 0), long_row=c.get("long_row", 0))
+        arr = (ctypes.c_void_p * len(tries))(*[t.h.value for t in tries])
+        h = ctypes.c_void_p()
+        _check(lib().eh_batch_create(self.ctx.h, arr, len(tries), QUERIES[query], ctypes.byref(e), ctypes.byref(h)))
+        self.h = h
+        self.ctx._adopt(self)
+
+    def run(self, stats=False):
+        res = np.zeros(len(self.tries), np.uint64)
+        st = QueryStats()
+        _check(lib().eh_batch_run(self.ctx.h, self.h, _ptr(res), ctypes.byref(st)))
+        if stats:
+            return res, {k: getattr(st, k) for k, _ in QueryStats._fields_}
+        return res
+
+    def free(self):
+        if getattr(self, "h", None):
+            lib().eh_batch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 def count_host_csr(head, off, vals, n_nodes, query="triangle", policy=HEURISTIC, model=None, ctx=None, stats=False,

@@ -313,6 +313,30 @@ eh_status eh_query_count_batched(eh_context* ctx, const eh_trie* const* tries, u
   });
 }
 
+eh_status eh_batch_create(eh_context* ctx, const eh_trie* const* tries, uint32_t n_tries, int query,
+                          const eh_exec_config* cfg, eh_batch** out) {
+  return guarded([&] {
+    need(ctx && tries && out, "null argument");
+    set_device(ctx);
+    *out = nullptr;
+    *out = batch_create(ctx, tries, n_tries, query, cfg);
+  });
+}
+
+eh_status eh_batch_run(eh_context* ctx, eh_batch* batch, uint64_t* results, eh_query_stats* stats) {
+  return guarded([&] {
+    need(ctx && batch && results, "null argument");
+    set_device(ctx);
+    batch_run(ctx, batch, results, stats);
+  });
+}
+
+eh_status eh_batch_free(eh_batch* batch) {
+  return guarded([&] {
+    if (batch) batch_free(batch);
+  });
+}
+
 eh_status eh_triangle_annotation(eh_context* ctx, const eh_trie* trie, const eh_exec_config* cfg, uint64_t* annot) {
   return guarded([&] {
     need(ctx && trie && annot, "null argument");

@@ -142,6 +142,10 @@ void query_count(eh_context* ctx, const eh_trie* t, int query, const eh_exec_con
 void query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query,
                          const eh_exec_config* cfg, uint64_t* results, eh_query_stats* stats);
 void triangle_annotation(eh_context* ctx, const eh_trie* t, const eh_exec_config* cfg, uint64_t* annot_dev);
+eh_batch* batch_create(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query,
+                       const eh_exec_config* cfg);
+void batch_run(eh_context* ctx, eh_batch* b, uint64_t* results, eh_query_stats* stats);
+void batch_free(eh_batch* b);
 
 // learned layout policy (eh_model.cu)
 void model_choose_layouts(eh_context* ctx, const eh_model* m, const eh_trie* t, uint64_t max_bitset_bytes,

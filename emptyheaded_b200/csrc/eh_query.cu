@@ -609,34 +609,50 @@ struct Launch {
 
 // Runs the intersection kernel of `query` over the concatenated plans of
 // n graphs; results accumulate into d_total[g].
-static Launch run_plans(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query, ExecParams ep,
-                        bool annot, unsigned long long* d_total, unsigned long long* d_annot, float* d_records,
-                        uint32_t* n_items_out, uint64_t* pairs_out) {
+// Everything a launch needs on the device, built once: the work plans of
+// the tries concatenated into one queue, their views, the launch shape.
+struct Prepared {
+  DevBuf<Item> items;
+  uint32_t n_items = 0;
+  uint64_t pairs = 0;
+  DevBuf<TrieView> dv;
+  DevBuf<RevView> dr;
+  DevBuf<unsigned int> q;
+  ExecParams ep{};
+  size_t smem = 0;
+  int grid = 1, threads = 32;
+  int query = 0;
+  bool annot = false;
+  uint32_t plan_launches = 0;
+};
+
+static void prepare(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query, ExecParams ep, bool annot,
+                    Prepared& P) {
   cudaStream_t s = ctx->stream;
-  Launch L;
+  P.query = query;
+  P.annot = annot;
   std::vector<Plan> plans(n);
   uint32_t total_items = 0;
   uint64_t pairs = 0;
   for (uint32_t g = 0; g < n; g++) {
     build_plan(ctx, tries[g], ep.chunk, g, plans[g]);
-    L.launches += plans[g].n ? 2 : 1;
+    P.plan_launches += plans[g].n ? 2 : 1;
     total_items += plans[g].n;
     pairs += tries[g]->rev_pairs;
   }
-  *n_items_out = total_items;
-  *pairs_out = pairs;
-  if (!total_items) return L;
-  DevBuf<Item> items;
-  const Item* items_p = plans[0].items.p;
-  if (n > 1) {
-    items.alloc(total_items, s);
+  P.n_items = total_items;
+  P.pairs = pairs;
+  if (n == 1) {
+    P.items = std::move(plans[0].items);
+  } else {
+    P.items.alloc(total_items ? total_items : 1, s);
     uint32_t o = 0;
     for (uint32_t g = 0; g < n; g++) {
       if (plans[g].n)
-        EH_CUDA(cudaMemcpyAsync(items.p + o, plans[g].items.p, plans[g].n * sizeof(Item), cudaMemcpyDeviceToDevice, s));
+        EH_CUDA(cudaMemcpyAsync(P.items.p + o, plans[g].items.p, plans[g].n * sizeof(Item), cudaMemcpyDeviceToDevice,
+                                s));
       o += plans[g].n;
     }
-    items_p = items.p;
   }
   std::vector<TrieView> hv(n);
   std::vector<RevView> hr(n);
@@ -644,50 +660,76 @@ static Launch run_plans(eh_context* ctx, const eh_trie* const* tries, uint32_t n
     hv[g] = tries[g]->view();
     hr[g] = rev_view(tries[g]);
   }
-  DevBuf<TrieView> dv(n, s);
-  DevBuf<RevView> dr(n, s);
-  DevBuf<unsigned int> q(2, s);
-  EH_CUDA(cudaMemcpyAsync(dv.p, hv.data(), n * sizeof(TrieView), cudaMemcpyHostToDevice, s));
-  EH_CUDA(cudaMemcpyAsync(dr.p, hr.data(), n * sizeof(RevView), cudaMemcpyHostToDevice, s));
-  EH_CUDA(cudaMemsetAsync(q.p, 0, 8, s));
-  QueryOut out{ep.shard_index, ep.shard_count, ep.long_row, d_total, d_annot, d_records, q.p, q.p + 1};
-  const int threads = 32 * ep.warps;
-  size_t smem = (size_t)ep.smem_words * 4 * ep.warps;
+  P.dv.alloc(n, s);
+  P.dr.alloc(n, s);
+  P.q.alloc(2, s);
+  EH_CUDA(cudaMemcpyAsync(P.dv.p, hv.data(), n * sizeof(TrieView), cudaMemcpyHostToDevice, s));
+  EH_CUDA(cudaMemcpyAsync(P.dr.p, hr.data(), n * sizeof(RevView), cudaMemcpyHostToDevice, s));
+  P.threads = 32 * ep.warps;
+  P.smem = (size_t)ep.smem_words * 4 * ep.warps;
   {
     int dev = 0, optin = 0;
     EH_CUDA(cudaGetDevice(&dev));
     EH_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    if (smem > (size_t)optin) {
+    if (P.smem > (size_t)optin) {
       // shrink the per-warp region to what a block may hold (a staged set
       // that no longer fits is probed in global memory instead)
       EH_REQUIRE(query != EH_QUERY_CLIQUE4, EH_ERR_UNSUPPORTED, "4-clique staging exceeds shared memory");
       ep.smem_words = (int)((optin / 4 / ep.warps) & ~1);
-      smem = (size_t)ep.smem_words * 4 * ep.warps;
+      P.smem = (size_t)ep.smem_words * 4 * ep.warps;
     }
   }
   const void* kfn;
   if (query == EH_QUERY_CLIQUE4) {
-    set_smem_attr(clique4_kernel, smem);
+    set_smem_attr(clique4_kernel, P.smem);
     kfn = (const void*)clique4_kernel;
   } else if (annot) {
-    set_smem_attr(triangle_kernel<true>, smem);
+    set_smem_attr(triangle_kernel<true>, P.smem);
     kfn = (const void*)triangle_kernel<true>;
   } else {
-    set_smem_attr(triangle_kernel<false>, smem);
+    set_smem_attr(triangle_kernel<false>, P.smem);
     kfn = (const void*)triangle_kernel<false>;
   }
-  const int per_sm = blocks_per_sm(kfn, threads, smem);
-  const int warps_total = num_sms() * per_sm * ep.warps;
-  const int grid = std::max(1, std::min(num_sms() * per_sm, (int)((total_items + ep.warps - 1) / ep.warps)));
-  (void)warps_total;
-  EH_CUDA(cudaEventRecord(ctx->ev1, s));
-  if (query == EH_QUERY_CLIQUE4)
-    clique4_kernel<<<grid, threads, smem, s>>>(dv.p, dr.p, items_p, total_items, ep.smem_words, out);
-  else if (annot)
-    triangle_kernel<true><<<grid, threads, smem, s>>>(dv.p, dr.p, items_p, total_items, ep.smem_words, out);
+  const int per_sm = blocks_per_sm(kfn, P.threads, P.smem);
+  P.grid = std::max(1, std::min(num_sms() * per_sm, (int)((total_items + ep.warps - 1) / ep.warps)));
+  P.ep = ep;
+  EH_CUDA(cudaStreamSynchronize(s));  // host staging vectors go out of scope
+}
+
+// Enqueue one run of a prepared launch: reset the queue, run the persistent
+// kernel.  No host synchronisation: capturable in a CUDA graph.
+static void launch(eh_context* ctx, Prepared& P, unsigned long long* d_total, unsigned long long* d_annot,
+                   float* d_records) {
+  cudaStream_t s = ctx->stream;
+  if (!P.n_items) return;
+  EH_CUDA(cudaMemsetAsync(P.q.p, 0, 8, s));
+  const ExecParams& ep = P.ep;
+  QueryOut out{ep.shard_index, ep.shard_count, ep.long_row, d_total, d_annot, d_records, P.q.p, P.q.p + 1};
+  if (P.query == EH_QUERY_CLIQUE4)
+    clique4_kernel<<<P.grid, P.threads, P.smem, s>>>(P.dv.p, P.dr.p, P.items.p, P.n_items, ep.smem_words, out);
+  else if (P.annot)
+    triangle_kernel<true><<<P.grid, P.threads, P.smem, s>>>(P.dv.p, P.dr.p, P.items.p, P.n_items, ep.smem_words,
+                                                            out);
   else
-    triangle_kernel<false><<<grid, threads, smem, s>>>(dv.p, dr.p, items_p, total_items, ep.smem_words, out);
+    triangle_kernel<false><<<P.grid, P.threads, P.smem, s>>>(P.dv.p, P.dr.p, P.items.p, P.n_items, ep.smem_words,
+                                                             out);
   EH_CHECK_LAUNCH();
+}
+
+// Plan + run + wait; the intersection kernel is timed with events.
+static Launch run_plans(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query, ExecParams ep,
+                        bool annot, unsigned long long* d_total, unsigned long long* d_annot, float* d_records,
+                        uint32_t* n_items_out, uint64_t* pairs_out) {
+  cudaStream_t s = ctx->stream;
+  Launch L;
+  Prepared P;
+  prepare(ctx, tries, n, query, ep, annot, P);
+  L.launches = P.plan_launches;
+  *n_items_out = P.n_items;
+  *pairs_out = P.pairs;
+  if (!P.n_items) return L;
+  EH_CUDA(cudaEventRecord(ctx->ev1, s));
+  launch(ctx, P, d_total, d_annot, d_records);
   EH_CUDA(cudaEventRecord(ctx->ev2, s));
   L.launches += 1;
   EH_CUDA(cudaEventSynchronize(ctx->ev2));
@@ -815,6 +857,112 @@ void triangle_annotation(eh_context* ctx, const eh_trie* t, const eh_exec_config
   run_plans(ctx, ts, 1, EH_QUERY_TRIANGLE, ep, true, dummy.p, (unsigned long long*)annot_dev, nullptr, &items,
             &pairs);
   EH_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace eh
+
+// ------------------------------------------------------------------ batches
+// A prepared batch: one queue over every trie's work items and the whole
+// step captured once as a CUDA graph (zero results, zero queue, persistent
+// kernel, results to pinned host memory).  A run is one graph launch.
+struct eh_batch {
+  eh_context* ctx = nullptr;
+  eh::Prepared P;
+  eh::DevBuf<unsigned long long> total;
+  unsigned long long* host = nullptr;  // pinned
+  std::vector<int> dirs;
+  uint32_t n = 0;
+  int query = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~eh_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (host) cudaFreeHost(host);
+  }
+};
+
+namespace eh {
+
+eh_batch* batch_create(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query,
+                       const eh_exec_config* cfg) {
+  cudaStream_t s = ctx->stream;
+  EH_REQUIRE(n > 0, EH_ERR_INVALID, "no tries");
+  EH_REQUIRE(query == EH_QUERY_TRIANGLE || query == EH_QUERY_CLIQUE4, EH_ERR_UNSUPPORTED,
+             "batches run the triangle or 4-clique plan");
+  ExecParams ep = exec_params(cfg);
+  for (uint32_t g = 0; g < n; g++) {
+    EH_REQUIRE(tries[g] && tries[g]->ctx == ctx, EH_ERR_INVALID, "null trie or trie of another context");
+    if (query == EH_QUERY_CLIQUE4) {
+      EH_REQUIRE(tries[g]->dir != DIR_GENERAL || tries[g]->rows == 0, EH_ERR_UNSUPPORTED,
+                 "4-clique needs a relation that is up-, down-oriented or symmetric");
+      const int need = 2 * ((int)tries[g]->info.max_set + 1);
+      if (ep.smem_words < need) ep.smem_words = (need + 1) & ~1;
+    }
+  }
+  auto* b = new eh_batch();
+  try {
+    b->ctx = ctx;
+    b->n = n;
+    b->query = query;
+    for (uint32_t g = 0; g < n; g++) b->dirs.push_back(tries[g]->dir);
+    prepare(ctx, tries, n, query, ep, false, b->P);
+    b->total.alloc(n, s);
+    EH_CUDA(cudaMallocHost((void**)&b->host, n * sizeof(unsigned long long)));
+    EH_CUDA(cudaStreamSynchronize(s));
+    EH_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaError_t cap = cudaSuccess;
+    try {
+      EH_CUDA(cudaMemsetAsync(b->total.p, 0, n * 8, s));
+      launch(ctx, b->P, b->total.p, nullptr, nullptr);
+      EH_CUDA(cudaMemcpyAsync(b->host, b->total.p, n * 8, cudaMemcpyDeviceToHost, s));
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(s, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    cap = cudaStreamEndCapture(s, &b->graph);
+    EH_CUDA(cap);
+    EH_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  } catch (...) {
+    delete b;
+    throw;
+  }
+  return b;
+}
+
+void batch_run(eh_context* ctx, eh_batch* b, uint64_t* results, eh_query_stats* stats) {
+  cudaStream_t s = ctx->stream;
+  EH_REQUIRE(b->ctx == ctx, EH_ERR_INVALID, "batch belongs to another context");
+  EH_CUDA(cudaEventRecord(ctx->ev0, s));
+  EH_CUDA(cudaGraphLaunch(b->exec, s));
+  EH_CUDA(cudaEventRecord(ctx->ev2, s));
+  EH_CUDA(cudaEventSynchronize(ctx->ev2));
+  float ms = 0;
+  EH_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev2));
+  for (uint32_t g = 0; g < b->n; g++) {
+    uint64_t v = b->host[g];
+    if (b->dirs[g] == DIR_SYM) v *= b->query == EH_QUERY_CLIQUE4 ? 24ull : 6ull;
+    results[g] = v;
+  }
+  if (stats) {
+    stats->query_ms = ms;
+    stats->kernel_ms = ms;
+    stats->launches = 1;
+    stats->work_items = b->P.n_items;
+    stats->wedges = b->P.pairs;
+    stats->algorithmic_bytes = 0;
+    stats->timed_out = 0;
+  }
+}
+
+void batch_free(eh_batch* b) {
+  cudaSetDevice(b->ctx->device);
+  cudaStream_t s = b->ctx->stream;
+  cudaStreamSynchronize(s);
+  delete b;
+  cudaStreamSynchronize(s);
 }
 
 }  // namespace eh

@@ -1,0 +1,29 @@
+"""Named synthetic workloads (seeded; no datasets are needed).
+
+rmat(scale)          R-MAT, edge factor 16, a/b/c/d = 0.57/0.19/0.19/0.05
+batch256()           256 independent R-MAT graphs, scale = round(exp(U(ln 10,
+                     ln 18))) from numpy's default_rng(2024), seed 1000 + i
+chunglu(n, ...)      Chung-Lu power law, symmetrised (barbell / lollipop)
+"""
+import numpy as np
+
+ABCD = (0.57, 0.19, 0.19)
+EDGE_FACTOR = 16
+
+
+def batch256_spec(n=256, seed=2024):
+    rng = np.random.default_rng(seed)
+    scales = np.rint(np.exp(rng.uniform(np.log(10), np.log(18), n))).astype(int)
+    return [(int(s), 1000 + i) for i, s in enumerate(scales)]
+
+
+def build_rmat_trie(E, scale, seed, ctx=None, symmetric=False, **trie_kw):
+    """Device pipeline: R-MAT samples -> encoded Edge relation -> trie."""
+    u, v = E.gen_rmat(seed, scale, EDGE_FACTOR << scale, *ABCD, ctx=ctx)
+    s, d, nodes = E.preprocess(u, v, symmetric=symmetric, ctx=ctx)
+    u.free()
+    v.free()
+    t = E.Trie(s, d, ctx=ctx, **trie_kw)
+    s.free()
+    d.free()
+    return t

@@ -198,6 +198,18 @@ eh_status eh_query_count(eh_context* ctx, const eh_trie* trie, int query, const 
 eh_status eh_query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t n_tries, int query,
                                  const eh_exec_config* cfg, uint64_t* results, eh_query_stats* stats);
 
+/* A prepared batch: the work plans of n tries (triangle or 4-clique)
+ * concatenated once into one queue, and the step (zero the results and the
+ * queue, the persistent kernel over every trie's items, the results to
+ * host) captured in a CUDA graph.  eh_batch_run replays the graph: one
+ * launch for the whole batch.  Same results as eh_query_count per trie.
+ * The tries must outlive the batch and not be re-laid-out while it exists. */
+typedef struct eh_batch eh_batch;
+eh_status eh_batch_create(eh_context* ctx, const eh_trie* const* tries, uint32_t n_tries, int query,
+                          const eh_exec_config* cfg, eh_batch** out);
+eh_status eh_batch_run(eh_context* ctx, eh_batch* batch, uint64_t* results, eh_query_stats* stats);
+eh_status eh_batch_free(eh_batch* batch);
+
 /* Per-head-entry triangle annotation T(a) (the annotated bag of
  * lollipop/barbell, TrieBuilder::set_annotation, TrieBuilder.cpp:428-446),
  * copied to host annot[n_head]. */

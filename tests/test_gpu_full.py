@@ -28,6 +28,21 @@ def test_rmat22_edge_list_is_the_reference_input(rmat22):
     assert hashlib.sha1(hs.tobytes() + hd.tobytes()).hexdigest() == g["sha1"]
 
 
+def test_rmat20_clique4_matches_reference(eh, golden):
+    """4-clique configuration: R-MAT scale 20, degree-ordered src < dst;
+    the reference engine counts 17,101,670,542."""
+    g = golden["synthetic"]["rmat_s20_ef16_s42"]
+    u, v = eh.gen_rmat(42, 20, 16 << 20)
+    s, d, nn = eh.preprocess(u, v)
+    hs, hd = s.numpy(), d.numpy()
+    assert hashlib.sha1(hs.tobytes() + hd.tobytes()).hexdigest() == g["sha1"]
+    t = eh.Trie(s, d)
+    assert t.count("clique4") == g["clique4"] == 17101670542
+    t.relayout(policy=2, forced=0, max_bitset_bytes=1 << 50)
+    assert t.count("clique4") == g["clique4"]
+    t.free()
+
+
 def test_rmat22_triangle_count_every_layout(eh, rmat22):
     s, d, nn, g = rmat22
     t = eh.Trie(s, d)
