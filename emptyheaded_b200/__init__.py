@@ -107,6 +107,8 @@ def lib():
             "eh_trie_set_bytes": [_P, ctypes.c_uint32, _P, ctypes.c_uint64, _u64p, ctypes.POINTER(ctypes.c_uint8)],
             "eh_set_intersect_batch": [_P, _P, _P, ctypes.c_uint32, _P, _P, _P, ctypes.c_uint32, _P, _P, _P],
             "eh_query_count": [_P, _P, ctypes.c_int, ctypes.POINTER(ExecConfig), _u64p, ctypes.POINTER(QueryStats)],
+            "eh_query_materialize": [_P, _P, ctypes.c_int, ctypes.POINTER(ExecConfig), ctypes.c_int, _P, _P, _P,
+                                     ctypes.c_uint64, _u64p],
             "eh_query_count_batched": [_P, _P, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ExecConfig), _P,
                                        ctypes.POINTER(QueryStats)],
             "eh_triangle_annotation": [_P, _P, ctypes.POINTER(ExecConfig), _P],
@@ -369,6 +371,24 @@ class Trie:
         if stats:
             return r.value, {k: getattr(st, k) for k, _ in QueryStats._fields_}
         return r.value
+
+    def materialize(self, query="triangle", project=False):
+        """Rows of Triangle(a,b,c) sorted by (a,b,c) as an (n, 3) uint32
+        array; project=True gives TriangleProj(a,b), an (n, 2) array."""
+        cols = 2 if project else 3
+        e = _exec_cfg()
+        n = ctypes.c_uint64()
+        # the device builds the rows once to size them, then fills
+        _check(lib().eh_query_materialize(self.ctx.h, self.h, QUERIES[query], ctypes.byref(e), cols, None, None,
+                                          None, 0, ctypes.byref(n)))
+        rows = n.value
+        a = np.empty(max(rows, 1), np.uint32)
+        b = np.empty(max(rows, 1), np.uint32)
+        c = np.empty(max(rows, 1), np.uint32)
+        _check(lib().eh_query_materialize(self.ctx.h, self.h, QUERIES[query], ctypes.byref(e), cols, _ptr(a),
+                                          _ptr(b), _ptr(c), rows, ctypes.byref(n)))
+        out = [a[:rows], b[:rows]] + ([] if project else [c[:rows]])
+        return np.stack(out, 1)
 
     def triangle_annotation(self):
         nh = self.info()["n_head"]

@@ -313,6 +313,15 @@ eh_status eh_query_count_batched(eh_context* ctx, const eh_trie* const* tries, u
   });
 }
 
+eh_status eh_query_materialize(eh_context* ctx, const eh_trie* trie, int query, const eh_exec_config* cfg,
+                               int n_cols, uint32_t* a, uint32_t* b, uint32_t* c, uint64_t cap, uint64_t* n_rows) {
+  return guarded([&] {
+    need(ctx && trie && n_rows, "null argument");
+    set_device(ctx);
+    query_materialize(ctx, trie, query, cfg, n_cols, a, b, c, cap, n_rows);
+  });
+}
+
 eh_status eh_batch_create(eh_context* ctx, const eh_trie* const* tries, uint32_t n_tries, int query,
                           const eh_exec_config* cfg, eh_batch** out) {
   return guarded([&] {

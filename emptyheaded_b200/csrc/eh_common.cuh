@@ -150,6 +150,9 @@ void exclusive_scan(const T* in, T* out, uint64_t n, T* total_dev, cudaStream_t 
 // LSD radix sort of n 64-bit keys on their low `bits` bits, in place
 // (tmp must hold n keys).
 void radix_sort_u64(uint64_t* keys, uint64_t* tmp, uint64_t n, int bits, cudaStream_t s);
+// The same with a uint32 payload per key, stable (vtmp holds n values).
+void radix_sort_kv(uint64_t* keys, uint64_t* ktmp, uint32_t* vals, uint32_t* vtmp, uint64_t n, int bits,
+                   cudaStream_t s);
 
 // Keep the first of each run of equal keys (keys sorted).  Writes the
 // compacted keys to out and the count to *count_host (synchronises).

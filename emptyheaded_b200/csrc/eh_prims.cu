@@ -124,11 +124,15 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint64_t
   counts[(uint64_t)threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
 }
 
+// kVals: a uint32 payload travels with each key (read at write time)
+template <bool kVals>
 __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint64_t* __restrict__ keys,
                                                                      uint64_t* __restrict__ out, uint64_t n,
                                                                      int shift,
                                                                      const uint32_t* __restrict__ offsets,
-                                                                     uint32_t tiles) {
+                                                                     uint32_t tiles,
+                                                                     const uint32_t* __restrict__ vin,
+                                                                     uint32_t* __restrict__ vout) {
   __shared__ uint32_t whist[kSortWarps][kRadix];
   __shared__ uint32_t tile_off[kRadix];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -173,30 +177,50 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint6
     const uint64_t i = wbase + (uint64_t)r * 32 + lane;
     if (i < n) {
       const uint32_t d = (uint32_t)((k[r] >> shift) & 0xff);
-      out[tile_off[d] + whist[wid][d] + pos[r]] = k[r];
+      const uint32_t dst = tile_off[d] + whist[wid][d] + pos[r];
+      out[dst] = k[r];
+      if (kVals) vout[dst] = vin[i];
     }
   }
 }
 
-void radix_sort_u64(uint64_t* keys, uint64_t* tmp, uint64_t n, int bits, cudaStream_t s) {
+// LSD passes; with vals != nullptr a uint32 payload follows its key (stable)
+static void radix_sort_impl(uint64_t* keys, uint64_t* tmp, uint32_t* vals, uint32_t* vtmp, uint64_t n, int bits,
+                            cudaStream_t s) {
   if (n < 2) return;
   EH_REQUIRE(n < (1ull << 32), EH_ERR_UNSUPPORTED, "radix sort supports fewer than 2^32 keys");
   const uint32_t tiles = (uint32_t)((n + kSortTile - 1) / kSortTile);
   DevBuf<uint32_t> counts((uint64_t)kRadix * tiles, s);
   uint64_t* src = keys;
   uint64_t* dst = tmp;
-  int passes = 0;
-  for (int shift = 0; shift < bits; shift += 8, passes++) {
+  uint32_t* vsrc = vals;
+  uint32_t* vdst = vtmp;
+  for (int shift = 0; shift < bits; shift += 8) {
     radix_hist_kernel<<<tiles, kSortThreads, 0, s>>>(src, n, shift, counts.p, tiles);
     EH_CHECK_LAUNCH();
     exclusive_scan<uint32_t>(counts.p, counts.p, (uint64_t)kRadix * tiles, nullptr, s);
-    radix_scatter_kernel<<<tiles, kSortThreads, 0, s>>>(src, dst, n, shift, counts.p, tiles);
+    if (vals)
+      radix_scatter_kernel<true><<<tiles, kSortThreads, 0, s>>>(src, dst, n, shift, counts.p, tiles, vsrc, vdst);
+    else
+      radix_scatter_kernel<false><<<tiles, kSortThreads, 0, s>>>(src, dst, n, shift, counts.p, tiles, nullptr,
+                                                                  nullptr);
     EH_CHECK_LAUNCH();
-    uint64_t* t = src;
-    src = dst;
-    dst = t;
+    std::swap(src, dst);
+    std::swap(vsrc, vdst);
   }
-  if (src != keys) EH_CUDA(cudaMemcpyAsync(keys, src, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+  if (src != keys) {
+    EH_CUDA(cudaMemcpyAsync(keys, src, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+    if (vals) EH_CUDA(cudaMemcpyAsync(vals, vsrc, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+  }
+}
+
+void radix_sort_u64(uint64_t* keys, uint64_t* tmp, uint64_t n, int bits, cudaStream_t s) {
+  radix_sort_impl(keys, tmp, nullptr, nullptr, n, bits, s);
+}
+
+void radix_sort_kv(uint64_t* keys, uint64_t* ktmp, uint32_t* vals, uint32_t* vtmp, uint64_t n, int bits,
+                   cudaStream_t s) {
+  radix_sort_impl(keys, ktmp, vals, vtmp, n, bits, s);
 }
 
 // ================================================================ unique

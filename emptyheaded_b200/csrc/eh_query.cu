@@ -34,6 +34,10 @@ namespace eh {
 constexpr int kMaxWarps = EH_TRI_MAX_THREADS / 32;  // per block
 constexpr int kDefaultWarps = kMaxWarps < 8 ? kMaxWarps : 8;
 constexpr uint32_t kDefaultLongRow = 32;  // rows with at least this many candidates run warp-wide
+#ifndef EH_LONG_UNROLL
+#define EH_LONG_UNROLL 4
+#endif
+constexpr int kLongUnroll = EH_LONG_UNROLL;  // independent candidate loads per lane per trip
 // Defaults measured on B200 at R-MAT-22 (4 KB of staging per warp leaves
 // room for 32 resident warps; 32K-probe items amortise staging); the
 // autotuner (emptyheaded_b200/autotune.py) re-picks them per trie.
@@ -186,10 +190,23 @@ __device__ __forceinline__ uint32_t probe(const Staged& s, uint32_t w) {
   }
 }
 
-// Stream the candidate ranges of rows [kb, ke) against the staged set,
-// flattening (row, element) pairs over the 32 lanes.  kAnnot adds each
-// hit to the annotation of the row's source (and, for symmetric tries,
-// of the matched element).
+// What a hit does besides counting: kMode 0 counts only; 1 adds it to the
+// annotation of the row's source (and, on a symmetric relation, of the
+// matched element) -- the annotated bag of TrieBuilder::set_annotation;
+// 2 writes the tuple (a, b, c) to the item's slice of the output columns
+// -- the materialized Triangle(a,b,c) of TrieBuilder::build_set.
+enum { MODE_COUNT = 0, MODE_ANNOT = 1, MODE_MAT = 2 };
+
+struct Sink {
+  unsigned long long* annot;  // MODE_ANNOT
+  uint32_t* ma;               // MODE_MAT: output columns
+  uint32_t* mb;
+  uint32_t* mc;
+  uint64_t base;              // MODE_MAT: first row of this item's slice
+  unsigned int* slot;         // MODE_MAT: the warp's running row count (shared)
+  uint32_t b;                 // MODE_MAT: value of the staged head entry b
+};
+
 // owner lane of flattened pair q: the number of lanes whose inclusive
 // prefix is <= q (q < total guarantees a result below 32)
 __device__ __forceinline__ uint32_t owner_lane(uint32_t incl, uint32_t q) {
@@ -202,14 +219,34 @@ __device__ __forceinline__ uint32_t owner_lane(uint32_t incl, uint32_t q) {
   return j;
 }
 
-template <bool kAnnot>
-__device__ __forceinline__ void annotate_hit(const TrieView& t, const RevView& r, unsigned long long* annot,
-                                             uint32_t src, uint32_t w) {
-  if (r.dir == DIR_SYM) {
-    atomicAdd(annot + src, 2ull);
-    atomicAdd(annot + __ldg(t.head_index + w), 2ull);
-  } else {
-    atomicAdd(annot + src, 1ull);
+template <int kMode>
+__device__ __forceinline__ void on_hit(const TrieView& t, const RevView& r, const Sink& sk, uint32_t src,
+                                       uint32_t w) {
+  if (kMode == MODE_ANNOT) {
+    if (r.dir == DIR_SYM) {
+      atomicAdd(sk.annot + src, 2ull);
+      atomicAdd(sk.annot + __ldg(t.head_index + w), 2ull);
+    } else {
+      atomicAdd(sk.annot + src, 1ull);
+    }
+  } else if (kMode == MODE_MAT) {
+    const uint32_t a = __ldg(t.head + src), b = sk.b;
+    if (r.dir == DIR_SYM) {
+      // one undirected triangle a < b < w stands for all 3! orderings
+      const uint64_t o = sk.base + atomicAdd(sk.slot, 6u);
+      const uint32_t p[6][3] = {{a, b, w}, {a, w, b}, {b, a, w}, {b, w, a}, {w, a, b}, {w, b, a}};
+#pragma unroll
+      for (int k = 0; k < 6; k++) {
+        sk.ma[o + k] = p[k][0];
+        sk.mb[o + k] = p[k][1];
+        sk.mc[o + k] = p[k][2];
+      }
+    } else {
+      const uint64_t o = sk.base + atomicAdd(sk.slot, 1u);
+      sk.ma[o] = a;
+      sk.mb[o] = b;
+      sk.mc[o] = w;
+    }
   }
 }
 
@@ -222,9 +259,9 @@ __device__ __forceinline__ void annotate_hit(const TrieView& t, const RevView& r
 // loads of N(a)'s words); the other rows are flattened (row, element)
 // pairs over the lanes, two pairs per lane per trip for memory-level
 // parallelism.
-template <int P, bool kAnnot>
+template <int P, int kMode>
 __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView& t, const RevView& r, uint32_t kb,
-                                                uint32_t ke, uint32_t long_row, unsigned long long* annot) {
+                                                uint32_t ke, uint32_t long_row, const Sink& sk) {
   constexpr bool kBits = (P == P_SBITS || P == P_GBITS);
   const uint32_t lane = lane_id();
   uint64_t cnt = 0;
@@ -234,7 +271,7 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
     if (k < ke) {
       lo = __ldg(r.rev_lo + k);
       len = __ldg(r.rev_hi + k) - lo;
-      if (kAnnot || kBits) src = __ldg(r.rev_src + k);
+      if (kMode != MODE_COUNT || kBits) src = __ldg(r.rev_src + k);
     }
     // ---- word rows
     if (kBits) {
@@ -272,10 +309,10 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
           const uint64_t bw = (P == P_SBITS) ? st.words[w - st.start] : __ldg(st.words + (w - st.start));
           uint64_t x = __ldg(t.bs_words + base + w) & bw & m;
           c += __popcll(x);
-          if (kAnnot) {
+          if (kMode != MODE_COUNT) {
             while (x) {
               const uint32_t bit = __ffsll((long long)x) - 1;
-              annotate_hit<kAnnot>(t, r, annot, src_j, (w << 6) | bit);
+              on_hit<kMode>(t, r, sk, src_j, (w << 6) | bit);
               x &= x - 1;
             }
           }
@@ -295,18 +332,19 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
         rows &= rows - 1;
         const uint32_t rlo = __shfl_sync(kFull, lo, j), rn = __shfl_sync(kFull, rlen, j);
         uint32_t src_j = 0;
-        if (kAnnot) src_j = __shfl_sync(kFull, src, j);
+        if (kMode != MODE_COUNT) src_j = __shfl_sync(kFull, src, j);
         const uint32_t* row = t.vals + rlo;
-        for (uint32_t i = lane; i < rn; i += 64) {
-          const bool second = i + 32 < rn;
-          const uint32_t w0 = __ldg(row + i);
-          const uint32_t w1 = second ? __ldg(row + i + 32) : 0;
-          const uint32_t h0 = probe<P>(st, w0);
-          const uint32_t h1 = second ? probe<P>(st, w1) : 0u;
-          cnt += h0 + h1;
-          if (kAnnot) {
-            if (h0) annotate_hit<kAnnot>(t, r, annot, src_j, w0);
-            if (h1) annotate_hit<kAnnot>(t, r, annot, src_j, w1);
+        for (uint32_t i = lane; i < rn; i += 32 * kLongUnroll) {
+          uint32_t w[kLongUnroll];
+#pragma unroll
+          for (int u = 0; u < kLongUnroll; u++) w[u] = (i + 32 * u < rn) ? __ldg(row + i + 32 * u) : 0u;
+#pragma unroll
+          for (int u = 0; u < kLongUnroll; u++) {
+            if (i + 32 * u < rn) {
+              const uint32_t h = probe<P>(st, w[u]);
+              cnt += h;
+              if (kMode != MODE_COUNT && h) on_hit<kMode>(t, r, sk, src_j, w[u]);
+            }
           }
         }
       }
@@ -321,7 +359,7 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
       const uint32_t lo0 = __shfl_sync(kFull, lo, j0), ex0 = __shfl_sync(kFull, excl, j0);
       const uint32_t lo1 = __shfl_sync(kFull, lo, j1), ex1 = __shfl_sync(kFull, excl, j1);
       uint32_t s0 = 0, s1 = 0;
-      if (kAnnot) {
+      if (kMode != MODE_COUNT) {
         s0 = __shfl_sync(kFull, src, j0);
         s1 = __shfl_sync(kFull, src, j1);
       }
@@ -330,9 +368,9 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
       const uint32_t h0 = q0 < total ? probe<P>(st, w0) : 0u;
       const uint32_t h1 = q1 < total ? probe<P>(st, w1) : 0u;
       cnt += h0 + h1;
-      if (kAnnot) {
-        if (h0) annotate_hit<kAnnot>(t, r, annot, s0, w0);
-        if (h1) annotate_hit<kAnnot>(t, r, annot, s1, w1);
+      if (kMode != MODE_COUNT) {
+        if (h0) on_hit<kMode>(t, r, sk, s0, w0);
+        if (h1) on_hit<kMode>(t, r, sk, s1, w1);
       }
     }
   }
@@ -385,14 +423,19 @@ struct QueryOut {
   float* records;              // per item timing records or null
   unsigned int* queue;         // atomic queue head
   unsigned int* error;         // set when a bound is hit
+  unsigned long long* item_counts;  // per item count x count_mult (materialize sizing) or null
+  uint32_t count_mult;
+  const unsigned long long* item_off;  // MODE_MAT: first output row of each item
+  uint32_t *ma, *mb, *mc;      // MODE_MAT: output columns
 };
 
-template <bool kAnnot>
+template <int kMode>
 __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict__ views,
                                                         const RevView* __restrict__ revs,
                                                         const Item* __restrict__ items, uint32_t n_items,
                                                         int cap_words, QueryOut out) {
   extern __shared__ uint32_t smem[];
+  __shared__ unsigned int slot[kMaxWarps];  // MODE_MAT: rows written by the warp's item so far
   const uint32_t lane = lane_id();
   const uint32_t wid = threadIdx.x >> 5;
   uint32_t* sm = smem + (size_t)wid * cap_words;
@@ -415,19 +458,26 @@ __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict_
     const RevView r = revs[item.g];
     long long t0 = 0;
     if (out.records && lane == 0) t0 = clock64();
+    Sink sk{out.annot, out.ma, out.mb, out.mc, 0, &slot[wid], 0};
+    if (kMode == MODE_MAT) {
+      if (lane == 0) slot[wid] = 0;
+      __syncwarp();
+      sk.base = out.item_off[it];
+      sk.b = t.head[item.hb];
+    }
     Staged st;
     const int mode = stage_set(t, item.hb, sm, cap_words, st);
-    unsigned long long* annot = kAnnot ? out.annot : nullptr;
     uint64_t c;
     switch (mode) {
-      case P_SBITS: c = stream_rows<P_SBITS, kAnnot>(st, t, r, item.kb, item.ke, out.long_row, annot); break;
-      case P_GBITS: c = stream_rows<P_GBITS, kAnnot>(st, t, r, item.kb, item.ke, out.long_row, annot); break;
-      case P_SLIST: c = stream_rows<P_SLIST, kAnnot>(st, t, r, item.kb, item.ke, out.long_row, annot); break;
-      case P_GLIST: c = stream_rows<P_GLIST, kAnnot>(st, t, r, item.kb, item.ke, out.long_row, annot); break;
-      default: c = stream_rows<P_GBLOCK, kAnnot>(st, t, r, item.kb, item.ke, out.long_row, annot); break;
+      case P_SBITS: c = stream_rows<P_SBITS, kMode>(st, t, r, item.kb, item.ke, out.long_row, sk); break;
+      case P_GBITS: c = stream_rows<P_GBITS, kMode>(st, t, r, item.kb, item.ke, out.long_row, sk); break;
+      case P_SLIST: c = stream_rows<P_SLIST, kMode>(st, t, r, item.kb, item.ke, out.long_row, sk); break;
+      case P_GLIST: c = stream_rows<P_GLIST, kMode>(st, t, r, item.kb, item.ke, out.long_row, sk); break;
+      default: c = stream_rows<P_GBLOCK, kMode>(st, t, r, item.kb, item.ke, out.long_row, sk); break;
     }
     c = warp_sum(c);
-    if (kAnnot && r.dir == DIR_SYM && lane == 0 && c) atomicAdd(out.annot + item.hb, 2ull * c);
+    if (kMode == MODE_ANNOT && r.dir == DIR_SYM && lane == 0 && c) atomicAdd(out.annot + item.hb, 2ull * c);
+    if (out.item_counts && lane == 0) out.item_counts[it] = c * out.count_mult;
     acc += c;
     __syncwarp();  // the staged region is reused by the next item
     if (out.records && lane == 0) {
@@ -684,11 +734,11 @@ static void prepare(eh_context* ctx, const eh_trie* const* tries, uint32_t n, in
     set_smem_attr(clique4_kernel, P.smem);
     kfn = (const void*)clique4_kernel;
   } else if (annot) {
-    set_smem_attr(triangle_kernel<true>, P.smem);
-    kfn = (const void*)triangle_kernel<true>;
+    set_smem_attr(triangle_kernel<MODE_ANNOT>, P.smem);
+    kfn = (const void*)triangle_kernel<MODE_ANNOT>;
   } else {
-    set_smem_attr(triangle_kernel<false>, P.smem);
-    kfn = (const void*)triangle_kernel<false>;
+    set_smem_attr(triangle_kernel<MODE_COUNT>, P.smem);
+    kfn = (const void*)triangle_kernel<MODE_COUNT>;
   }
   const int per_sm = blocks_per_sm(kfn, P.threads, P.smem);
   P.grid = std::max(1, std::min(num_sms() * per_sm, (int)((total_items + ep.warps - 1) / ep.warps)));
@@ -708,10 +758,10 @@ static void launch(eh_context* ctx, Prepared& P, unsigned long long* d_total, un
   if (P.query == EH_QUERY_CLIQUE4)
     clique4_kernel<<<P.grid, P.threads, P.smem, s>>>(P.dv.p, P.dr.p, P.items.p, P.n_items, ep.smem_words, out);
   else if (P.annot)
-    triangle_kernel<true><<<P.grid, P.threads, P.smem, s>>>(P.dv.p, P.dr.p, P.items.p, P.n_items, ep.smem_words,
+    triangle_kernel<MODE_ANNOT><<<P.grid, P.threads, P.smem, s>>>(P.dv.p, P.dr.p, P.items.p, P.n_items, ep.smem_words,
                                                             out);
   else
-    triangle_kernel<false><<<P.grid, P.threads, P.smem, s>>>(P.dv.p, P.dr.p, P.items.p, P.n_items, ep.smem_words,
+    triangle_kernel<MODE_COUNT><<<P.grid, P.threads, P.smem, s>>>(P.dv.p, P.dr.p, P.items.p, P.n_items, ep.smem_words,
                                                              out);
   EH_CHECK_LAUNCH();
 }
@@ -856,6 +906,161 @@ void triangle_annotation(eh_context* ctx, const eh_trie* t, const eh_exec_config
   const eh_trie* ts[1] = {t};
   run_plans(ctx, ts, 1, EH_QUERY_TRIANGLE, ep, true, dummy.p, (unsigned long long*)annot_dev, nullptr, &items,
             &pairs);
+  EH_CUDA(cudaStreamSynchronize(s));
+}
+
+// ------------------------------------------------------------ materialize
+// Triangle(a,b,c) :- Edge(a,b),Edge(b,c),Edge(a,c) as tuples sorted by
+// (a,b,c): the rows Trie::foreach (Trie.cpp:130-160) yields on the
+// reference's materialized output trie (TrieBuilder::build_set /
+// allocate_next / set_level, TrieBuilder.cpp:44-221, 376-410).  One counting
+// run sizes every work item's slice, a second run writes the tuples into
+// the slices, and two stable key-value radix sorts (by c, then by (a,b))
+// order them.
+__global__ void iota_kernel(uint32_t* __restrict__ v, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    v[i] = (uint32_t)i;
+}
+__global__ void widen_kernel(const uint32_t* __restrict__ c, uint64_t n, uint64_t* __restrict__ k) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    k[i] = c[i];
+}
+// keys2[i] = a[idx[i]] << bb | b[idx[i]], vals2[i] = c value (keys1[i])
+__global__ void ab_key_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                              const uint32_t* __restrict__ idx, const uint64_t* __restrict__ csorted, uint64_t n,
+                              int bb, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t j = idx[i];
+    keys[i] = ((uint64_t)a[j] << bb) | b[j];
+    vals[i] = (uint32_t)csorted[i];
+  }
+}
+__global__ void split_ab_kernel(const uint64_t* __restrict__ keys, uint64_t n, int bb, uint32_t* __restrict__ a,
+                                uint32_t* __restrict__ b) {
+  const uint64_t mask = (1ull << bb) - 1;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    a[i] = (uint32_t)(keys[i] >> bb);
+    b[i] = (uint32_t)(keys[i] & mask);
+  }
+}
+
+// TriangleProj(a,b): the reference's plan drops attributes that are neither
+// materialized, selected nor aggregated (codegen/query/QueryPlan.scala:245),
+// so c is never intersected: the rows are (a,b) with b in N(a) ∩ head, in
+// trie order.  One flag + scan + compact over the rows.
+__global__ void proj_flag_kernel(TrieView t, uint32_t* __restrict__ flag) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < t.rows; e += (uint64_t)gridDim.x * blockDim.x)
+    flag[e] = __ldg(t.head_index + t.vals[e]) >= 0 ? 1u : 0u;
+}
+__global__ void proj_write_kernel(TrieView t, const uint32_t* __restrict__ seg, const uint32_t* __restrict__ pos,
+                                  uint32_t* __restrict__ a, uint32_t* __restrict__ b) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < t.rows; e += (uint64_t)gridDim.x * blockDim.x)
+    if (__ldg(t.head_index + t.vals[e]) >= 0) {
+      a[pos[e]] = t.head[seg[e]];
+      b[pos[e]] = t.vals[e];
+    }
+}
+__global__ void seg_of_rows_kernel(const uint64_t* __restrict__ off, uint32_t nh, uint32_t* __restrict__ seg) {
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = warp; i < nh; i += nwarps)
+    for (uint64_t e = off[i] + lane; e < off[i + 1]; e += 32) seg[e] = i;
+}
+
+static void query_project_ab(eh_context* ctx, const eh_trie* t, uint32_t* ha, uint32_t* hb, uint64_t cap,
+                             uint64_t* n_rows) {
+  cudaStream_t s = ctx->stream;
+  *n_rows = 0;
+  if (!t->rows) return;
+  const int grid = num_sms() * 8;
+  DevBuf<uint32_t> pos(t->rows, s), seg(t->rows, s), tot(1, s);
+  proj_flag_kernel<<<grid, 256, 0, s>>>(t->view(), pos.p);
+  EH_CHECK_LAUNCH();
+  exclusive_scan<uint32_t>(pos.p, pos.p, t->rows, tot.p, s);
+  uint32_t m = 0;
+  EH_CUDA(cudaMemcpyAsync(&m, tot.p, 4, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaStreamSynchronize(s));
+  *n_rows = m;
+  if (!ha || !hb || !m) return;
+  EH_REQUIRE(cap >= m, EH_ERR_INVALID, "output columns hold fewer rows than the result");
+  DevBuf<uint32_t> da(m, s), db(m, s);
+  seg_of_rows_kernel<<<grid, 256, 0, s>>>(t->off.p, t->n_head, seg.p);
+  proj_write_kernel<<<grid, 256, 0, s>>>(t->view(), seg.p, pos.p, da.p, db.p);
+  EH_CHECK_LAUNCH();
+  EH_CUDA(cudaMemcpyAsync(ha, da.p, (size_t)m * 4, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaMemcpyAsync(hb, db.p, (size_t)m * 4, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaStreamSynchronize(s));
+}
+
+void query_materialize(eh_context* ctx, const eh_trie* t, int query, const eh_exec_config* cfg, int n_cols,
+                       uint32_t* ha, uint32_t* hb, uint32_t* hc, uint64_t cap, uint64_t* n_rows) {
+  cudaStream_t s = ctx->stream;
+  EH_REQUIRE(query == EH_QUERY_TRIANGLE, EH_ERR_UNSUPPORTED, "materialized output is built for the triangle plan");
+  EH_REQUIRE(n_cols == 2 || n_cols == 3, EH_ERR_INVALID, "n_cols must be 3 (a,b,c) or 2 (projection on a,b)");
+  EH_REQUIRE(t->ctx == ctx, EH_ERR_INVALID, "trie belongs to another context");
+  if (n_cols == 2) {
+    query_project_ab(ctx, t, ha, hb, cap, n_rows);
+    return;
+  }
+  uint64_t n = 0;
+  query_count(ctx, t, EH_QUERY_TRIANGLE, cfg, &n, nullptr);
+  *n_rows = n;
+  if (n == 0 || !ha || !hb || !hc) return;  // the row count is the triangle count
+  EH_REQUIRE(cap >= n, EH_ERR_INVALID, "output columns hold fewer rows than the result");
+  EH_REQUIRE(n < (1ull << 32), EH_ERR_UNSUPPORTED, "materialized results hold fewer than 2^32 rows");
+  ExecParams ep = exec_params(cfg);
+  ep.shard_index = 0;
+  ep.shard_count = 1;
+  Prepared P;
+  const eh_trie* ts[1] = {t};
+  prepare(ctx, ts, 1, EH_QUERY_TRIANGLE, ep, false, P);
+  set_smem_attr(triangle_kernel<MODE_MAT>, P.smem);
+  DevBuf<unsigned long long> counts(P.n_items ? P.n_items : 1, s), offs(P.n_items ? P.n_items : 1, s),
+      total(1, s), rows(1, s);
+  EH_CUDA(cudaMemsetAsync(total.p, 0, 8, s));
+  const uint32_t mult = t->dir == DIR_SYM ? 6u : 1u;
+  QueryOut out{0, 1, P.ep.long_row, total.p, nullptr, nullptr, P.q.p, P.q.p + 1};
+  out.item_counts = counts.p;
+  out.count_mult = mult;
+  EH_CUDA(cudaMemsetAsync(P.q.p, 0, 8, s));
+  triangle_kernel<MODE_COUNT><<<P.grid, P.threads, P.smem, s>>>(P.dv.p, P.dr.p, P.items.p, P.n_items,
+                                                                P.ep.smem_words, out);
+  EH_CHECK_LAUNCH();
+  exclusive_scan<uint64_t>((const uint64_t*)counts.p, (uint64_t*)offs.p, P.n_items, (uint64_t*)rows.p, s);
+  uint64_t nr = 0;
+  EH_CUDA(cudaMemcpyAsync(&nr, rows.p, 8, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaStreamSynchronize(s));
+  EH_REQUIRE(nr == n, EH_ERR_CUDA, "materialize: counting runs disagree");
+  DevBuf<uint32_t> ma(n, s), mb(n, s), mc(n, s);
+  out.item_counts = nullptr;
+  out.item_off = offs.p;
+  out.ma = ma.p;
+  out.mb = mb.p;
+  out.mc = mc.p;
+  EH_CUDA(cudaMemsetAsync(P.q.p, 0, 8, s));
+  triangle_kernel<MODE_MAT><<<P.grid, P.threads, P.smem, s>>>(P.dv.p, P.dr.p, P.items.p, P.n_items,
+                                                              P.ep.smem_words, out);
+  EH_CHECK_LAUNCH();
+  // order by (a, b, c): stable sort by c, then stable sort by (a, b)
+  const int grid = num_sms() * 8;
+  const int bb = bits_for(t->n_nodes ? t->n_nodes - 1 : 0);
+  DevBuf<uint64_t> k1(n, s), k1t(n, s);
+  DevBuf<uint32_t> idx(n, s), idxt(n, s);
+  widen_kernel<<<grid, 256, 0, s>>>(mc.p, n, k1.p);
+  iota_kernel<<<grid, 256, 0, s>>>(idx.p, n);
+  EH_CHECK_LAUNCH();
+  radix_sort_kv(k1.p, k1t.p, idx.p, idxt.p, n, bb, s);
+  DevBuf<uint64_t> k2(n, s);
+  DevBuf<uint32_t> v2(n, s);
+  ab_key_kernel<<<grid, 256, 0, s>>>(ma.p, mb.p, idx.p, k1.p, n, bb, k2.p, v2.p);
+  EH_CHECK_LAUNCH();
+  radix_sort_kv(k2.p, k1t.p, v2.p, idxt.p, n, 2 * bb, s);
+  split_ab_kernel<<<grid, 256, 0, s>>>(k2.p, n, bb, ma.p, mb.p);
+  EH_CHECK_LAUNCH();
+  EH_CUDA(cudaMemcpyAsync(ha, ma.p, n * 4, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaMemcpyAsync(hb, mb.p, n * 4, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaMemcpyAsync(hc, v2.p, n * 4, cudaMemcpyDeviceToHost, s));
   EH_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -206,6 +206,26 @@ __global__ void wedge_kernel(TrieView t, uint64_t* __restrict__ wedges) {
   }
 }
 
+// red[0] = largest set, red[1] = sum of squared set sizes
+__global__ void set_size_stats_kernel(const uint64_t* __restrict__ off, uint32_t nh, unsigned long long* red) {
+  unsigned long long mx = 0, sq = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nh; i += gridDim.x * blockDim.x) {
+    const unsigned long long d = off[i + 1] - off[i];
+    mx = d > mx ? d : mx;
+    sq += d * d;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long m2 = __shfl_xor_sync(kFull, mx, o);
+    mx = m2 > mx ? m2 : mx;
+  }
+  sq = warp_sum(sq);
+  if (lane_id() == 0) {
+    atomicMax(&red[0], mx);
+    atomicAdd(&red[1], sq);
+  }
+}
+
 __global__ void layout_hist_kernel(const uint8_t* __restrict__ layout, uint32_t n, uint32_t* __restrict__ hist) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     atomicAdd(&hist[layout[i] & 3], 1u);
@@ -317,19 +337,19 @@ void trie_build_from_csr(eh_context* ctx, eh_trie* t) {
   t->info.rows = t->rows;
   t->info.n_head = t->n_head;
   t->info.n_nodes = t->n_nodes;
-  // largest set
+  // largest set and sum of squared set sizes
   uint32_t mx = 0;
+  t->sum_sq_deg = 0;
   if (t->n_head) {
-    std::vector<uint64_t> h(t->n_head + 1);
-    EH_CUDA(cudaMemcpyAsync(h.data(), t->off.p, (t->n_head + 1) * 8, cudaMemcpyDeviceToHost, s));
+    DevBuf<unsigned long long> red(2, s);
+    EH_CUDA(cudaMemsetAsync(red.p, 0, 16, s));
+    set_size_stats_kernel<<<grid, 256, 0, s>>>(t->off.p, t->n_head, red.p);
+    EH_CHECK_LAUNCH();
+    unsigned long long h[2];
+    EH_CUDA(cudaMemcpyAsync(h, red.p, 16, cudaMemcpyDeviceToHost, s));
     EH_CUDA(cudaStreamSynchronize(s));
-    uint64_t sq = 0;
-    for (uint32_t i = 0; i < t->n_head; i++) {
-      const uint64_t d = h[i + 1] - h[i];
-      mx = std::max<uint32_t>(mx, (uint32_t)d);
-      sq += d * d;
-    }
-    t->sum_sq_deg = sq;
+    mx = (uint32_t)h[0];
+    t->sum_sq_deg = h[1];
   }
   t->info.max_set = mx;
   trie_build_reverse(ctx, t);
@@ -391,6 +411,7 @@ __global__ void seg_kernel(const uint64_t* __restrict__ off, uint32_t nh, uint32
 
 // counts rows that are not "up" (b <= a), not "down" (b >= a), rows (a,b)
 // whose mirror (b,a) is absent, and self-loops
+template <bool kMirror>
 __global__ void direction_kernel(TrieView t, const uint32_t* __restrict__ seg, unsigned long long* __restrict__ cnt) {
   unsigned long long not_up = 0, not_down = 0, no_mirror = 0, loops = 0;
   for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < t.rows; e += (uint64_t)gridDim.x * blockDim.x) {
@@ -398,6 +419,7 @@ __global__ void direction_kernel(TrieView t, const uint32_t* __restrict__ seg, u
     not_up += b <= a;
     not_down += b >= a;
     loops += a == b;
+    if (!kMirror) continue;
     const int32_t hb = t.head_index[b];
     bool found = false;
     if (hb >= 0) {
@@ -430,8 +452,11 @@ __device__ __forceinline__ void rev_range(int dir, uint64_t e, uint64_t a_lo, ui
   else { lo = a_lo; hi = a_hi; }
 }
 
-__global__ void rev_key_kernel(TrieView t, const uint32_t* __restrict__ seg, int dir, int br,
-                               uint64_t sentinel, uint64_t* __restrict__ keys, uint32_t* __restrict__ cnt) {
+// key = head position of b (sentinel for rows the plans never read),
+// payload = the row; rows arrive in row order, so a stable sort on the key
+// alone leaves each b's rows in row order
+__global__ void rev_key_kernel(TrieView t, const uint32_t* __restrict__ seg, int dir, uint64_t sentinel,
+                               uint64_t* __restrict__ keys, uint32_t* __restrict__ rowid, uint32_t* __restrict__ cnt) {
   for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < t.rows; e += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t ha = seg[e];
     const uint32_t a = t.head[ha], b = t.vals[e];
@@ -439,18 +464,23 @@ __global__ void rev_key_kernel(TrieView t, const uint32_t* __restrict__ seg, int
     uint64_t lo, hi;
     rev_range(dir, e, t.off[ha], t.off[ha + 1], lo, hi);
     const bool keep = hb >= 0 && hi > lo && (dir != DIR_SYM || a < b);
-    keys[e] = keep ? (((uint64_t)hb << br) | e) : sentinel;
+    keys[e] = keep ? (uint64_t)hb : sentinel;
+    rowid[e] = (uint32_t)e;
     if (keep) atomicAdd(&cnt[hb], 1u);
   }
 }
 
-__global__ void rev_fill_kernel(TrieView t, const uint32_t* __restrict__ seg, int dir, int br,
-                                const uint64_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ lo_out,
+__global__ void widen_u32_kernel(const uint32_t* __restrict__ in, uint64_t n, uint64_t* __restrict__ out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = in[i];
+}
+
+__global__ void rev_fill_kernel(TrieView t, const uint32_t* __restrict__ seg, int dir,
+                                const uint32_t* __restrict__ rowid, uint64_t n, uint32_t* __restrict__ lo_out,
                                 uint32_t* __restrict__ hi_out, uint32_t* __restrict__ src_out,
                                 uint64_t* __restrict__ work) {
-  const uint64_t mask = (1ull << br) - 1;
   for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t e = keys[k] & mask;
+    const uint64_t e = rowid[k];
     const uint32_t ha = seg[e];
     uint64_t lo, hi;
     rev_range(dir, e, t.off[ha], t.off[ha + 1], lo, hi);
@@ -478,46 +508,58 @@ void trie_build_reverse(eh_context* ctx, eh_trie* t) {
   DevBuf<uint32_t> seg(t->rows, s);
   seg_kernel<<<grid, 256, 0, s>>>(t->off.p, t->n_head, seg.p);
   EH_CHECK_LAUNCH();
+  // direction: up / down from one cheap pass; the mirror search only when
+  // the relation is neither
   DevBuf<unsigned long long> cnt(4, s);
   EH_CUDA(cudaMemsetAsync(cnt.p, 0, 32, s));
-  direction_kernel<<<grid, 256, 0, s>>>(t->view(), seg.p, cnt.p);
+  direction_kernel<false><<<grid, 256, 0, s>>>(t->view(), seg.p, cnt.p);
   EH_CHECK_LAUNCH();
   unsigned long long c[4];
   EH_CUDA(cudaMemcpyAsync(c, cnt.p, 32, cudaMemcpyDeviceToHost, s));
   EH_CUDA(cudaStreamSynchronize(s));
-  // a symmetric relation takes the oriented schedule (each undirected
-  // triangle once, times 3!) only without self-loops
-  t->dir = c[0] == 0 ? DIR_UP : c[1] == 0 ? DIR_DOWN : (c[2] == 0 && c[3] == 0) ? DIR_SYM : DIR_GENERAL;
-
-  const int br = bits_for(t->rows);
+  if (c[0] == 0) {
+    t->dir = DIR_UP;
+  } else if (c[1] == 0) {
+    t->dir = DIR_DOWN;
+  } else {
+    EH_CUDA(cudaMemsetAsync(cnt.p, 0, 32, s));
+    direction_kernel<true><<<grid, 256, 0, s>>>(t->view(), seg.p, cnt.p);
+    EH_CHECK_LAUNCH();
+    EH_CUDA(cudaMemcpyAsync(c, cnt.p, 32, cudaMemcpyDeviceToHost, s));
+    EH_CUDA(cudaStreamSynchronize(s));
+    // a symmetric relation takes the oriented schedule (each undirected
+    // triangle once, times 3!) only without self-loops
+    t->dir = (c[2] == 0 && c[3] == 0) ? DIR_SYM : DIR_GENERAL;
+  }
+  // group the rows a->b the plans read by b (stable: row order within b)
   const int bh = bits_for(t->n_head);
-  const uint64_t sentinel = (bh + br >= 64) ? ~0ull : ((1ull << (bh + br)) - 1);
-  DevBuf<uint64_t> keys(t->rows, s), tmp(t->rows, s);
+  const uint64_t sentinel = (1ull << bh) - 1;  // above every head position
+  DevBuf<uint64_t> keys(t->rows, s), ktmp(t->rows, s);
+  DevBuf<uint32_t> rowid(t->rows, s), vtmp(t->rows, s);
   DevBuf<uint32_t> per(t->n_head + 1, s);
   EH_CUDA(cudaMemsetAsync(per.p, 0, (t->n_head + 1) * 4, s));
-  rev_key_kernel<<<grid, 256, 0, s>>>(t->view(), seg.p, t->dir, br, sentinel, keys.p, per.p);
+  rev_key_kernel<<<grid, 256, 0, s>>>(t->view(), seg.p, t->dir, sentinel, keys.p, rowid.p, per.p);
   EH_CHECK_LAUNCH();
-  radix_sort_u64(keys.p, tmp.p, t->rows, bh + br, s);
-  DevBuf<uint32_t> per_scan(t->n_head + 1, s), tot(1, s);
-  exclusive_scan<uint32_t>(per.p, per_scan.p, t->n_head + 1, tot.p, s);
-  uint32_t n = 0;
-  EH_CUDA(cudaMemcpyAsync(&n, tot.p, 4, cudaMemcpyDeviceToHost, s));
-  EH_CUDA(cudaStreamSynchronize(s));
-  t->rev_entries = n;
-  // widen the per-head offsets to 64 bits
-  std::vector<uint32_t> h32(t->n_head + 1);
-  std::vector<uint64_t> h64(t->n_head + 1);
-  EH_CUDA(cudaMemcpyAsync(h32.data(), per_scan.p, (t->n_head + 1) * 4, cudaMemcpyDeviceToHost, s));
-  EH_CUDA(cudaStreamSynchronize(s));
-  for (uint32_t i = 0; i <= t->n_head; i++) h64[i] = h32[i];
-  EH_CUDA(cudaMemcpyAsync(t->rev_off.p, h64.data(), (t->n_head + 1) * 8, cudaMemcpyHostToDevice, s));
+  radix_sort_kv(keys.p, ktmp.p, rowid.p, vtmp.p, t->rows, bh, s);
+  {
+    DevBuf<uint64_t> per64(t->n_head + 1, s);
+    widen_u32_kernel<<<grid, 256, 0, s>>>(per.p, t->n_head + 1, per64.p);
+    EH_CHECK_LAUNCH();
+    DevBuf<uint64_t> tot(1, s);
+    exclusive_scan<uint64_t>(per64.p, t->rev_off.p, t->n_head + 1, tot.p, s);
+    uint64_t n64 = 0;
+    EH_CUDA(cudaMemcpyAsync(&n64, tot.p, 8, cudaMemcpyDeviceToHost, s));
+    EH_CUDA(cudaStreamSynchronize(s));
+    t->rev_entries = n64;
+  }
+  const uint64_t n = t->rev_entries;
   t->rev_lo.alloc(n ? n : 1, s);
   t->rev_hi.alloc(n ? n : 1, s);
   t->rev_src.alloc(n ? n : 1, s);
   t->rev_wpre.alloc(n + 1, s);
   EH_CUDA(cudaMemsetAsync(t->rev_wpre.p, 0, (n + 1) * 8, s));
   if (n) {
-    rev_fill_kernel<<<grid, 256, 0, s>>>(t->view(), seg.p, t->dir, br, keys.p, n, t->rev_lo.p, t->rev_hi.p,
+    rev_fill_kernel<<<grid, 256, 0, s>>>(t->view(), seg.p, t->dir, rowid.p, n, t->rev_lo.p, t->rev_hi.p,
                                          t->rev_src.p, t->rev_wpre.p);
     EH_CHECK_LAUNCH();
     exclusive_scan<uint64_t>(t->rev_wpre.p, t->rev_wpre.p, n, t->rev_wpre.p + n, s);

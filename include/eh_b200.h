@@ -193,6 +193,20 @@ typedef struct {
 eh_status eh_query_count(eh_context* ctx, const eh_trie* trie, int query, const eh_exec_config* cfg,
                          uint64_t* result, eh_query_stats* stats);
 
+/* Materialized output of the triangle plan, rows sorted lexicographically
+ * (the order Trie::foreach, storage_engine/src/Trie.cpp:130-160, walks the
+ * reference's output trie).  Replaces the materializing bag of
+ * Triangle(a,b,c) :- Edge(a,b),Edge(b,c),Edge(a,c) (TrieBuilder::build_set /
+ * allocate_next / set_level, storage_engine/src/TrieBuilder.cpp:44-221,
+ * 376-410).  n_cols == 3: rows (a,b,c) in a, b, c; n_cols == 2: the
+ * projection TriangleProj(a,b) as the reference plans it -- attributes
+ * neither materialized, selected nor aggregated are dropped
+ * (query_compiler/.../codegen/query/QueryPlan.scala:245), so the rows are
+ * (a,b) with b in N(a) ∩ head (c unused).  Host columns of cap rows; with
+ * a == NULL only *n_rows is returned. */
+eh_status eh_query_materialize(eh_context* ctx, const eh_trie* trie, int query, const eh_exec_config* cfg,
+                               int n_cols, uint32_t* a, uint32_t* b, uint32_t* c, uint64_t cap, uint64_t* n_rows);
+
 /* Same plan over many tries in one persistent launch; results[g] per
  * trie. */
 eh_status eh_query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t n_tries, int query,

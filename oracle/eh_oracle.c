@@ -370,6 +370,31 @@ uint64_t eho_triangle(const uint32_t* head, uint32_t nh, const uint64_t* off, co
   return t;
 }
 
+/* Triangle(a,b,c) materialized: the generated loop nest visits a in head
+ * order, b in N(a) ∩ head in order, c in N(a) ∩ N(b) in order, so the
+ * tuples come out sorted by (a,b,c) (the output trie's Trie::foreach
+ * order).  Writes at most cap tuples; returns the total. */
+uint64_t eho_triangle_list(const uint32_t* head, uint32_t nh, const uint64_t* off, const uint32_t* vals, uint32_t* a,
+                           uint32_t* b, uint32_t* c, uint64_t cap) {
+  uint64_t n = 0;
+  uint32_t* tmp = NULL;
+  uint64_t tcap = 0;
+  for (uint32_t ia = 0; ia < nh; ia++) {
+    const uint32_t* na = vals + off[ia];
+    const uint64_t da = off[ia + 1] - off[ia];
+    if (da > tcap) { free(tmp); tcap = da; tmp = (uint32_t*)malloc(tcap * sizeof(uint32_t)); }
+    for (uint64_t j = 0; j < da; j++) {
+      int64_t ib = head_find(head, nh, na[j]);
+      if (ib < 0) continue;
+      const uint64_t k = eho_intersect(vals + off[ib], off[ib + 1] - off[ib], na, da, tmp);
+      for (uint64_t q = 0; q < k; q++, n++)
+        if (n < cap) { a[n] = head[ia]; b[n] = na[j]; c[n] = tmp[q]; }
+    }
+  }
+  free(tmp);
+  return n;
+}
+
 /* FliqueAgg plan (order [a,b,c,d]): N-way intersections chain pairwise,
  * smallest input first (TrieBuilder.cpp:276-348).  Here: S = N(a) ∩ N(b)
  * restricted to head, then d ∈ S ∩ N(c). */

@@ -64,6 +64,9 @@ uint64_t eho_intersect(const uint32_t* a, uint64_t na, const uint32_t* b, uint64
  * accumulated modulo 2^64 (the reference accumulates in signed long). */
 uint64_t eho_triangle(const uint32_t* head, uint32_t nh, const uint64_t* off, const uint32_t* vals);
 uint64_t eho_clique4(const uint32_t* head, uint32_t nh, const uint64_t* off, const uint32_t* vals);
+/* Triangle(a,b,c) tuples in (a,b,c) order; at most cap written, total returned */
+uint64_t eho_triangle_list(const uint32_t* head, uint32_t nh, const uint64_t* off, const uint32_t* vals, uint32_t* a,
+                           uint32_t* b, uint32_t* c, uint64_t cap);
 /* T(a) = number of ordered (b,c) closing a triangle at a; per head entry */
 void eho_triangle_annot(const uint32_t* head, uint32_t nh, const uint64_t* off, const uint32_t* vals,
                         uint64_t* T);

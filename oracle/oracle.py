@@ -73,6 +73,8 @@ def lib():
             f.restype = ctypes.c_uint64
             f.argtypes = [_u32p, ctypes.c_uint32, _u64p, _u32p]
         L.eho_triangle_per_vertex.argtypes = [_u32p, ctypes.c_uint32, _u64p, _u32p, _u64p]
+        L.eho_triangle_list.restype = ctypes.c_uint64
+        L.eho_triangle_list.argtypes = [_u32p, ctypes.c_uint32, _u64p, _u32p, _u32p, _u32p, _u32p, ctypes.c_uint64]
         L.eho_triangle_annot.argtypes = [_u32p, ctypes.c_uint32, _u64p, _u32p, _u64p]
         L.eho_mlp_loss_grad.restype = ctypes.c_double
         L.eho_mlp_loss_grad.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int), _f64p, _f64p, _f64p,
@@ -171,6 +173,28 @@ class Trie:
 
     def barbell(self):
         return int(lib().eho_barbell(*self._args()))
+
+    def triangle_tuples(self):
+        """Triangle(a,b,c) rows in (a,b,c) order, as an (n, 3) uint32 array."""
+        L = lib()
+        n = int(L.eho_triangle_list(*self._args(), np.zeros(1, np.uint32), np.zeros(1, np.uint32),
+                                    np.zeros(1, np.uint32), 0))
+        a = np.empty(max(n, 1), np.uint32)
+        b = np.empty(max(n, 1), np.uint32)
+        c = np.empty(max(n, 1), np.uint32)
+        L.eho_triangle_list(*self._args(), a, b, c, n)
+        return np.stack([a[:n], b[:n], c[:n]], 1)
+
+    def triangle_projection(self):
+        """TriangleProj(a,b) :- Edge(a,b),Edge(b,c),Edge(a,c) as the
+        reference plans it: attributes that are neither materialized,
+        selected nor aggregated are dropped from the loop nest
+        (query_compiler/.../codegen/query/QueryPlan.scala:245), so c is never
+        intersected and the rows are (a,b) with b in N(a) ∩ head, in trie
+        order."""
+        a = np.repeat(self.head, np.diff(self.off).astype(np.int64))
+        keep = np.isin(self.vals, self.head)
+        return np.stack([a[keep], self.vals[keep]], 1)
 
     def triangle_per_vertex(self):
         per = np.empty(max(1, self.n_head), np.uint64)

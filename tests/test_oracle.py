@@ -133,3 +133,18 @@ def test_mlp_gradient_finite_difference(oracle):
         lm, _ = oracle.mlp_loss_grad(dims, q, x, y)
         fd = (lp - lm) / (2 * eps)
         assert abs(fd - g[k]) <= 1e-6 + 1e-5 * abs(fd), (k, fd, g[k])
+
+
+def test_triangle_listing_goldens(oracle, facebook):
+    """Triangle(a,b,c) and TriangleProj(a,b) on facebook_pruned:
+    1612010 rows with row0 (6,5,2), 85658 rows with row0 (6,5)
+    (test/graph/travis.py:282-318)."""
+    p = facebook["pruned"]
+    t = oracle.Trie(p[:, 0], p[:, 1])
+    rows = t.triangle_tuples()
+    assert len(rows) == 1612010 and tuple(rows[0]) == (6, 5, 2)
+    proj = t.triangle_projection()
+    assert len(proj) == 85658 and tuple(proj[0]) == (6, 5)
+    # the projected attribute c is not intersected by the reference plan:
+    # more rows than the pairs that close a triangle
+    assert len(np.unique(rows[:, :2], axis=0)) == 84185
