@@ -107,6 +107,7 @@ def lib():
             "eh_trie_set_bytes": [_P, ctypes.c_uint32, _P, ctypes.c_uint64, _u64p, ctypes.POINTER(ctypes.c_uint8)],
             "eh_set_intersect_batch": [_P, _P, _P, ctypes.c_uint32, _P, _P, _P, ctypes.c_uint32, _P, _P, _P],
             "eh_query_count": [_P, _P, ctypes.c_int, ctypes.POINTER(ExecConfig), _u64p, ctypes.POINTER(QueryStats)],
+            "eh_query_count_noalloc": [_P, _P, ctypes.c_int, ctypes.POINTER(ExecConfig), _u64p],
             "eh_query_materialize": [_P, _P, ctypes.c_int, ctypes.POINTER(ExecConfig), ctypes.c_int, _P, _P, _P,
                                      ctypes.c_uint64, _u64p],
             "eh_query_count_batched": [_P, _P, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ExecConfig), _P,

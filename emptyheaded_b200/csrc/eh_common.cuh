@@ -146,6 +146,11 @@ inline int bits_for(uint64_t maxv) {
 // the total through *total_dev when non-null (device pointer, one T).
 template <typename T>
 void exclusive_scan(const T* in, T* out, uint64_t n, T* total_dev, cudaStream_t s);
+// The same with its tile sums in caller memory; allocates nothing.
+uint64_t scan_scratch_elems(uint64_t n);
+template <typename T>
+void exclusive_scan_scratch(const T* in, T* out, uint64_t n, T* total_dev, T* scratch, uint64_t scratch_elems,
+                            cudaStream_t s);
 
 // LSD radix sort of n 64-bit keys on their low `bits` bits, in place
 // (tmp must hold n keys).

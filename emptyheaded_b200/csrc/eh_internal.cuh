@@ -146,6 +146,8 @@ eh_batch* batch_create(eh_context* ctx, const eh_trie* const* tries, uint32_t n,
                        const eh_exec_config* cfg);
 void batch_run(eh_context* ctx, eh_batch* b, uint64_t* results, eh_query_stats* stats);
 void batch_free(eh_batch* b);
+void query_count_in_scratch(eh_context* ctx, const eh_trie* t, int query, const eh_exec_config* cfg,
+                            unsigned char* scratch, size_t bytes, uint64_t* result);
 void query_materialize(eh_context* ctx, const eh_trie* t, int query, const eh_exec_config* cfg, int n_cols,
                        uint32_t* a, uint32_t* b, uint32_t* c, uint64_t cap, uint64_t* n_rows);
 

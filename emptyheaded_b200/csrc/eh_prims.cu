@@ -97,6 +97,42 @@ void exclusive_scan(const T* in, T* out, uint64_t n, T* total_dev, cudaStream_t 
 template void exclusive_scan<uint32_t>(const uint32_t*, uint32_t*, uint64_t, uint32_t*, cudaStream_t);
 template void exclusive_scan<uint64_t>(const uint64_t*, uint64_t*, uint64_t, uint64_t*, cudaStream_t);
 
+// Tile-sum elements exclusive_scan_scratch needs for n inputs (all levels).
+uint64_t scan_scratch_elems(uint64_t n) {
+  uint64_t need = 0;
+  while (n > (uint64_t)kScanTile) {
+    n = (n + kScanTile - 1) / kScanTile;
+    need += n;
+  }
+  return need;
+}
+
+// exclusive_scan with its tile sums in caller memory (scratch_elems >=
+// scan_scratch_elems(n)): allocates nothing.
+template <typename T>
+void exclusive_scan_scratch(const T* in, T* out, uint64_t n, T* total_dev, T* scratch, uint64_t scratch_elems,
+                            cudaStream_t s) {
+  if (n == 0) {
+    if (total_dev) EH_CUDA(cudaMemsetAsync(total_dev, 0, sizeof(T), s));
+    return;
+  }
+  const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+  if (tiles == 1) {
+    scan_tile_kernel<T><<<1, kScanThreads, 0, s>>>(in, out, n, nullptr, total_dev);
+    EH_CHECK_LAUNCH();
+    return;
+  }
+  EH_REQUIRE(scratch_elems >= tiles, EH_ERR_INVALID, "scan scratch too small");
+  T* sums = scratch;
+  scan_reduce_kernel<T><<<(unsigned)tiles, kScanThreads, 0, s>>>(in, n, sums);
+  EH_CHECK_LAUNCH();
+  exclusive_scan_scratch<T>(sums, sums, tiles, nullptr, scratch + tiles, scratch_elems - tiles, s);
+  scan_tile_kernel<T><<<(unsigned)tiles, kScanThreads, 0, s>>>(in, out, n, sums, total_dev);
+  EH_CHECK_LAUNCH();
+}
+template void exclusive_scan_scratch<uint32_t>(const uint32_t*, uint32_t*, uint64_t, uint32_t*, uint32_t*, uint64_t,
+                                               cudaStream_t);
+
 // ============================================================ radix sort
 // LSD, 8-bit digits.  One pass = histogram per tile (digit-major counters),
 // exclusive scan of the counters, stable scatter.  A tile is 8 warps x 16

@@ -1064,6 +1064,101 @@ void query_materialize(eh_context* ctx, const eh_trie* t, int query, const eh_ex
   EH_CUDA(cudaStreamSynchronize(s));
 }
 
+// One triangle / 4-clique COUNT of one trie with every piece of device
+// scratch (queue, total, views, planner arrays, scan tile sums, work items)
+// carved out of `scratch` (256-byte aligned, `bytes` long): allocates
+// nothing.  Throws EH_ERR_UNSUPPORTED when the trie needs more scratch.
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+void query_count_in_scratch(eh_context* ctx, const eh_trie* t, int query, const eh_exec_config* cfg,
+                            unsigned char* scratch, size_t bytes, uint64_t* result) {
+  cudaStream_t s = ctx->stream;
+  EH_REQUIRE(query == EH_QUERY_TRIANGLE || query == EH_QUERY_CLIQUE4, EH_ERR_UNSUPPORTED,
+             "the allocation-free path runs the triangle and 4-clique plans");
+  EH_REQUIRE(t->ctx == ctx, EH_ERR_INVALID, "trie belongs to another context");
+  ExecParams ep = exec_params(cfg);
+  EH_REQUIRE(ep.shard_count == 1, EH_ERR_UNSUPPORTED, "the allocation-free path runs unsharded");
+  if (query == EH_QUERY_CLIQUE4) {
+    EH_REQUIRE(t->dir != DIR_GENERAL || t->rows == 0, EH_ERR_UNSUPPORTED,
+               "4-clique needs a relation that is up-, down-oriented or symmetric");
+    const int need = 2 * ((int)t->info.max_set + 1);
+    if (ep.smem_words < need) ep.smem_words = (need + 1) & ~1;
+    EH_REQUIRE((size_t)ep.smem_words * 4 * ep.warps <= 200 * 1024, EH_ERR_UNSUPPORTED,
+               "4-clique: largest set too large for the shared-memory staging");
+  }
+  // carve the scratch
+  const uint32_t nh = t->n_head;
+  const uint64_t scan_elems = scan_scratch_elems(nh);
+  const size_t off_ctrl = 0;  // u32 queue, u32 error, u64 total
+  const size_t off_tv = 256;
+  const size_t off_rv = align256(off_tv + sizeof(TrieView));
+  const size_t off_nitems = align256(off_rv + sizeof(RevView));
+  const size_t off_ipos = align256(off_nitems + 4ull * nh);
+  const size_t off_tot = align256(off_ipos + 4ull * nh);
+  const size_t off_scan = align256(off_tot + 4);
+  const size_t off_items = align256(off_scan + 4ull * scan_elems);
+  EH_REQUIRE(off_items <= bytes, EH_ERR_UNSUPPORTED,
+             "trie too large for the allocation-free path: its planner needs " + std::to_string(off_items) +
+                 " bytes of scratch before the work items, the path holds " + std::to_string(bytes));
+  unsigned int* queue = reinterpret_cast<unsigned int*>(scratch + off_ctrl);
+  unsigned long long* total = reinterpret_cast<unsigned long long*>(scratch + off_ctrl + 8);
+  TrieView* dv = reinterpret_cast<TrieView*>(scratch + off_tv);
+  RevView* dr = reinterpret_cast<RevView*>(scratch + off_rv);
+  uint32_t* nitems = reinterpret_cast<uint32_t*>(scratch + off_nitems);
+  uint32_t* ipos = reinterpret_cast<uint32_t*>(scratch + off_ipos);
+  uint32_t* tot = reinterpret_cast<uint32_t*>(scratch + off_tot);
+  uint32_t* scan_tmp = reinterpret_cast<uint32_t*>(scratch + off_scan);
+  Item* items = reinterpret_cast<Item*>(scratch + off_items);
+  // the array keeps the previous call's contents: zero what must start at 0
+  EH_CUDA(cudaMemsetAsync(scratch + off_ctrl, 0, 16, s));
+  const TrieView hv = t->view();
+  const RevView hr = rev_view(t);
+  EH_CUDA(cudaMemcpyAsync(dv, &hv, sizeof(TrieView), cudaMemcpyHostToDevice, s));
+  EH_CUDA(cudaMemcpyAsync(dr, &hr, sizeof(RevView), cudaMemcpyHostToDevice, s));
+  uint32_t n_items = 0;
+  if (t->rev_entries) {
+    const int pgrid = num_sms() * 4;
+    plan_count_kernel<<<pgrid, 256, 0, s>>>(hr, nh, ep.chunk, nitems);
+    EH_CHECK_LAUNCH();
+    exclusive_scan_scratch<uint32_t>(nitems, ipos, nh, tot, scan_tmp, scan_elems, s);
+    EH_CUDA(cudaMemcpyAsync(&n_items, tot, 4, cudaMemcpyDeviceToHost, s));
+    EH_CUDA(cudaStreamSynchronize(s));
+    EH_REQUIRE(off_items + sizeof(Item) * (size_t)n_items <= bytes, EH_ERR_UNSUPPORTED,
+               "trie too large for the allocation-free path: it needs " +
+                   std::to_string(off_items + sizeof(Item) * (size_t)n_items) + " bytes of scratch, the path holds " +
+                   std::to_string(bytes));
+    if (n_items) {
+      plan_fill_kernel<<<pgrid, 256, 0, s>>>(hr, nh, nitems, ipos, n_items, 0, items);
+      EH_CHECK_LAUNCH();
+    }
+  }
+  if (n_items) {
+    const int threads = 32 * ep.warps;
+    const size_t smem = (size_t)ep.smem_words * 4 * ep.warps;
+    int dev = 0, optin = 0;
+    EH_CUDA(cudaGetDevice(&dev));
+    EH_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    EH_REQUIRE(smem <= (size_t)optin, EH_ERR_INVALID, "shared staging above the per-block limit");
+    const void* kfn = query == EH_QUERY_CLIQUE4 ? (const void*)clique4_kernel : (const void*)triangle_kernel<MODE_COUNT>;
+    if (query == EH_QUERY_CLIQUE4) set_smem_attr(clique4_kernel, smem);
+    else set_smem_attr(triangle_kernel<MODE_COUNT>, smem);
+    const int per_sm = blocks_per_sm(kfn, threads, smem);
+    const int grid = std::max(1, std::min(num_sms() * per_sm, (int)((n_items + ep.warps - 1) / ep.warps)));
+    QueryOut out{0, 1, ep.long_row, total, nullptr, nullptr, queue, queue + 1};
+    if (query == EH_QUERY_CLIQUE4)
+      clique4_kernel<<<grid, threads, smem, s>>>(dv, dr, items, n_items, ep.smem_words, out);
+    else
+      triangle_kernel<MODE_COUNT><<<grid, threads, smem, s>>>(dv, dr, items, n_items, ep.smem_words, out);
+    EH_CHECK_LAUNCH();
+  }
+  unsigned long long h = 0;
+  EH_CUDA(cudaMemcpyAsync(&h, total, 8, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaStreamSynchronize(s));
+  uint64_t v = h;
+  if (t->dir == DIR_SYM) v *= query == EH_QUERY_CLIQUE4 ? 24ull : 6ull;
+  *result = v;
+}
+
 }  // namespace eh
 
 // ------------------------------------------------------------------ batches

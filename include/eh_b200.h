@@ -193,6 +193,21 @@ typedef struct {
 eh_status eh_query_count(eh_context* ctx, const eh_trie* trie, int query, const eh_exec_config* cfg,
                          uint64_t* result, eh_query_stats* stats);
 
+/* eh_query_count for callers that must not allocate device memory while
+ * they query (an embedding host whose device memory belongs to another
+ * allocator, where a library cudaMalloc could fail and a cudaFree would
+ * synchronise the device under the host's own work).  No counterpart in
+ * the reference.  Runs the triangle or 4-clique plan with all its scratch
+ * (work plan, queue, result) in one fixed 64 MiB device array compiled into
+ * the library; calls no cudaMalloc/cudaFree.  Limit: the trie's plan must
+ * fit, about 8 bytes per head entry plus 16 per work item (an R-MAT
+ * scale-22 trie fits); larger tries get EH_ERR_UNSUPPORTED.  The first call
+ * on a device looks the array up (make it before any stream capture).  Calls
+ * share the array: this entry serialises its own calls per device; other
+ * GPU work touching the array concurrently would race. */
+eh_status eh_query_count_noalloc(eh_context* ctx, const eh_trie* trie, int query, const eh_exec_config* cfg,
+                                 uint64_t* result);
+
 /* Materialized output of the triangle plan, rows sorted lexicographically
  * (the order Trie::foreach, storage_engine/src/Trie.cpp:130-160, walks the
  * reference's output trie).  Replaces the materializing bag of
