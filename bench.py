@@ -158,12 +158,14 @@ def load_peaks():
 
 
 def profile_traffic():
-    """Per-launch DRAM bytes of the intersection kernel from the committed
-    ncu summary (profiles/triangle_kernel_rmat22.json), if present."""
-    p = os.path.join(ROOT, "profiles", "triangle_kernel_rmat22.json")
+    """Per-launch DRAM bytes (read + write) of the intersection kernel from
+    the committed one-pass ncu capture at this workload
+    (profiles/triangle_kernel_rmat22_dram.json), if present."""
+    p = os.path.join(ROOT, "profiles", "triangle_kernel_rmat22_dram.json")
     if os.path.exists(p):
         with open(p) as f:
-            return json.load(f).get("dram_bytes_per_launch")
+            d = json.load(f)
+        return int(d["dram_bytes_read"]) + int(d["dram_bytes_write"])
     return None
 
 
