@@ -33,6 +33,8 @@ STATUS_NAMES = {1: "INVALID", 2: "CUDA", 3: "OOM", 4: "TIMEOUT", 5: "UNSUPPORTED
 RANGE_BITSET, UINTEGER, BLOCK_BITSET = 0, 1, 3
 HEURISTIC, LEARNED, FORCED = 0, 1, 2
 QUERIES = {"triangle": 0, "clique4": 1, "lollipop": 2, "barbell": 3}
+# equality-selection plans (Trie.count_select)
+SELECT_QUERIES = {"clique4_sel": 4, "barbell_sel": 5}
 
 
 class EHError(RuntimeError):
@@ -106,8 +108,16 @@ def lib():
             "eh_trie_export": [_P, _P, _P, _P, _P],
             "eh_trie_set_bytes": [_P, ctypes.c_uint32, _P, ctypes.c_uint64, _u64p, ctypes.POINTER(ctypes.c_uint8)],
             "eh_set_intersect_batch": [_P, _P, _P, ctypes.c_uint32, _P, _P, _P, ctypes.c_uint32, _P, _P, _P],
+            "eh_encoding_build": [_P, _P, _P, ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_P)],
+            "eh_encoding_encode": [_P, _P, _P, ctypes.c_uint64, ctypes.c_int, _P],
+            "eh_encoding_decode": [_P, _P, _P, ctypes.c_uint64, ctypes.c_int, _P],
+            "eh_encoding_size": [_P, _u64p],
+            "eh_encoding_values": [_P, _P, _P, ctypes.c_uint64],
+            "eh_encoding_free": [_P],
             "eh_query_count": [_P, _P, ctypes.c_int, ctypes.POINTER(ExecConfig), _u64p, ctypes.POINTER(QueryStats)],
             "eh_query_count_noalloc": [_P, _P, ctypes.c_int, ctypes.POINTER(ExecConfig), _u64p],
+            "eh_query_count_select": [_P, _P, ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ExecConfig), _u64p,
+                                      ctypes.POINTER(QueryStats)],
             "eh_query_materialize": [_P, _P, ctypes.c_int, ctypes.POINTER(ExecConfig), ctypes.c_int, _P, _P, _P,
                                      ctypes.c_uint64, _u64p],
             "eh_query_count_batched": [_P, _P, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ExecConfig), _P,
@@ -373,6 +383,22 @@ class Trie:
             return r.value, {k: getattr(st, k) for k, _ in QueryStats._fields_}
         return r.value
 
+    def count_select(self, query, value, stats=False, config=None):
+        """FliqueSelAgg (query="clique4_sel", Edge(a,x), x=value) or
+        BarbellSelAgg (query="barbell_sel", Edge(a,p), Edge(p,x), p=value):
+        the reference's equality-selection COUNT queries.  Raises when value
+        is in neither column of the relation."""
+        config = config or {}
+        e = _exec_cfg(config.get("warps", 0), config.get("chunk", 0), config.get("smem_words", 0), False, (0, 1),
+                      config.get("long_row", 0))
+        r = ctypes.c_uint64()
+        st = QueryStats()
+        _check(lib().eh_query_count_select(self.ctx.h, self.h, SELECT_QUERIES[query], int(value), ctypes.byref(e),
+                                           ctypes.byref(r), ctypes.byref(st)))
+        if stats:
+            return r.value, {k: getattr(st, k) for k, _ in QueryStats._fields_}
+        return r.value
+
     def materialize(self, query="triangle", project=False):
         """Rows of Triangle(a,b,c) sorted by (a,b,c) as an (n, 3) uint32
         array; project=True gives TriangleProj(a,b), an (n, 2) array."""
@@ -509,6 +535,66 @@ def set_intersect(sets, layouts, pairs, materialize=False, ctx=None):
 
 
 # -------------------------------------------------------------------- model
+VALUE_TYPES = {"uint32": (0, np.uint32), "int32": (1, np.int32), "int64": (2, np.int64), "float32": (3, np.float32)}
+
+
+class Encoding:
+    """Dictionary encoding on the device, the reference's Encoding<T>
+    (storage_engine/src/Encoding.cpp:21-48): keys in ascending value order
+    over the distinct values of all the given columns.  value_type is one of
+    "uint32", "int32", "int64", "float32" (uint32_t, int, long, float)."""
+
+    def __init__(self, cols, value_type="uint32", ctx=None):
+        self.ctx = ctx or default_context()
+        self.value_type = value_type
+        code, dt = VALUE_TYPES[value_type]
+        self._dt = dt
+        cols = [np.ascontiguousarray(c, dt) for c in cols]
+        ptrs = (ctypes.c_void_p * max(1, len(cols)))(*[c.ctypes.data for c in cols])
+        lens = np.array([len(c) for c in cols] or [0], np.uint64)
+        h = ctypes.c_void_p()
+        _check(lib().eh_encoding_build(self.ctx.h, ptrs, _ptr(lens), len(cols), code, 0, ctypes.byref(h)))
+        self.h = h.value
+        self.ctx._adopt(self)
+
+    def __len__(self):
+        n = ctypes.c_uint64()
+        _check(lib().eh_encoding_size(self.h, ctypes.byref(n)))
+        return n.value
+
+    def encode(self, col):
+        """encode_column: uint32 keys (raises for a value not in the encoding)"""
+        col = np.ascontiguousarray(col, self._dt)
+        keys = np.empty(max(1, len(col)), np.uint32)
+        _check(lib().eh_encoding_encode(self.ctx.h, self.h, col.ctypes.data, len(col), 0, _ptr(keys)))
+        return keys[: len(col)]
+
+    def decode(self, keys):
+        """key_to_value per key"""
+        keys = np.ascontiguousarray(keys, np.uint32)
+        out = np.empty(max(1, len(keys)), self._dt)
+        _check(lib().eh_encoding_decode(self.ctx.h, self.h, _ptr(keys), len(keys), 0, out.ctypes.data))
+        return out[: len(keys)]
+
+    def values(self):
+        """the key_to_value table"""
+        n = len(self)
+        out = np.empty(max(1, n), self._dt)
+        _check(lib().eh_encoding_values(self.ctx.h, self.h, out.ctypes.data, n))
+        return out[:n]
+
+    def free(self):
+        if getattr(self, "h", None):
+            lib().eh_encoding_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 class Model:
     """Small fp32 MLP trained and evaluated by the engine's own kernels."""
 

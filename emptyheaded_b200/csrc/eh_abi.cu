@@ -1,6 +1,9 @@
 // C ABI entry points (declared in include/eh_b200.h).  Every call catches
 // its own failures and returns a status; nothing here aborts the process.
+#include <chrono>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "eh_internal.cuh"
@@ -8,6 +11,63 @@
 namespace eh {
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[kMaxPoolDevices] = {};
+}  // namespace
+
+cudaMemPool_t device_pool() {
+  int dev = 0;
+  EH_CUDA(cudaGetDevice(&dev));
+  EH_REQUIRE(dev >= 0 && dev < kMaxPoolDevices, EH_ERR_UNSUPPORTED, "device index too large");
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    EH_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = ~0ull;  // keep freed blocks for reuse until trimmed
+    EH_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pools[dev] = pool;
+  }
+  return g_pools[dev];
+}
+
+bool trace_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("EH_TRACE");
+    return e && *e && strcmp(e, "0") != 0;
+  }();
+  return on;
+}
+
+static double wall_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+TracePhase::TracePhase(const char* n, cudaStream_t st) : name(n), s(st), on(trace_enabled()) {
+  if (!on) return;
+  cudaStreamSynchronize(s);
+  t0 = wall_ms();
+}
+
+void TracePhase::end() {
+  if (!on) return;
+  on = false;
+  cudaStreamSynchronize(s);
+  fprintf(stderr, "eh-trace %-24s %9.3f ms\n", name, wall_ms() - t0);
+}
+
+void trim_device_pool(int device) {
+  if (device < 0 || device >= kMaxPoolDevices) return;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (g_pools[device]) cudaMemPoolTrimTo(g_pools[device], 0);
+}
 
 eh_model* model_create(eh_context* ctx, int n_layers, const int* dims, uint64_t seed);
 float model_train(eh_model* m, const float* x, const float* y, uint32_t batch, float lr, uint32_t steps);
@@ -84,6 +144,7 @@ eh_status eh_context_destroy(eh_context* ctx) {
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->ev2) cudaEventDestroy(ctx->ev2);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    trim_device_pool(ctx->device);  // return the pool's unused blocks to the driver
     delete ctx;
   });
 }
@@ -108,7 +169,7 @@ eh_status eh_device_alloc(eh_context* ctx, uint64_t bytes, void** out) {
     set_device(ctx);
     *out = nullptr;
     if (!bytes) return;
-    cudaError_t e = cudaMallocAsync(out, bytes, ctx->stream);
+    cudaError_t e = cudaMallocFromPoolAsync(out, bytes, device_pool(), ctx->stream);
     if (e != cudaSuccess) {
       cudaGetLastError();
       *out = nullptr;
@@ -142,8 +203,8 @@ static void alloc_pair(eh_context* ctx, uint64_t m, uint32_t** u, uint32_t** v) 
   need(u && v, "null output");
   *u = *v = nullptr;
   if (!m) return;
-  if (cudaMallocAsync((void**)u, m * 4, ctx->stream) != cudaSuccess ||
-      cudaMallocAsync((void**)v, m * 4, ctx->stream) != cudaSuccess) {
+  if (cudaMallocFromPoolAsync((void**)u, m * 4, device_pool(), ctx->stream) != cudaSuccess ||
+      cudaMallocFromPoolAsync((void**)v, m * 4, device_pool(), ctx->stream) != cudaSuccess) {
     cudaGetLastError();
     if (*u) cudaFreeAsync(*u, ctx->stream);
     *u = *v = nullptr;
@@ -304,6 +365,68 @@ eh_status eh_query_count(eh_context* ctx, const eh_trie* trie, int query, const 
   });
 }
 
+eh_status eh_encoding_build(eh_context* ctx, const void* const* cols, const uint64_t* n_rows, uint32_t n_cols,
+                            int value_type, int on_device, eh_encoding** out) {
+  return guarded([&] {
+    need(ctx && out && (n_cols == 0 || (cols && n_rows)), "null argument");
+    *out = nullptr;
+    set_device(ctx);
+    *out = encoding_build(ctx, cols, n_rows, n_cols, value_type, on_device);
+  });
+}
+
+eh_status eh_encoding_encode(eh_context* ctx, const eh_encoding* enc, const void* col, uint64_t n, int on_device,
+                             uint32_t* keys) {
+  return guarded([&] {
+    need(ctx && enc && (n == 0 || (col && keys)), "null argument");
+    need(encoding_ctx(enc) == ctx, "encoding belongs to another context");
+    set_device(ctx);
+    encoding_encode(ctx, enc, col, n, on_device, keys);
+  });
+}
+
+eh_status eh_encoding_decode(eh_context* ctx, const eh_encoding* enc, const uint32_t* keys, uint64_t n,
+                             int on_device, void* values) {
+  return guarded([&] {
+    need(ctx && enc && (n == 0 || (keys && values)), "null argument");
+    need(encoding_ctx(enc) == ctx, "encoding belongs to another context");
+    set_device(ctx);
+    encoding_decode(ctx, enc, keys, n, on_device, values);
+  });
+}
+
+eh_status eh_encoding_size(const eh_encoding* enc, uint64_t* n_distinct) {
+  return guarded([&] {
+    need(enc && n_distinct, "null argument");
+    *n_distinct = encoding_size(enc);
+  });
+}
+
+eh_status eh_encoding_values(eh_context* ctx, const eh_encoding* enc, void* values, uint64_t cap) {
+  return guarded([&] {
+    need(ctx && enc && (cap == 0 || values), "null argument");
+    need(encoding_ctx(enc) == ctx, "encoding belongs to another context");
+    set_device(ctx);
+    encoding_values(ctx, enc, values, cap);
+  });
+}
+
+eh_status eh_encoding_free(eh_encoding* enc) {
+  return guarded([&] {
+    if (!enc) return;
+    encoding_free(enc);
+  });
+}
+
+eh_status eh_query_count_select(eh_context* ctx, const eh_trie* trie, int query, uint32_t value,
+                                const eh_exec_config* cfg, uint64_t* result, eh_query_stats* stats) {
+  return guarded([&] {
+    need(ctx && trie && result, "null argument");
+    set_device(ctx);
+    query_count_select(ctx, trie, query, value, cfg, result, stats);
+  });
+}
+
 eh_status eh_query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t n_tries, int query,
                                  const eh_exec_config* cfg, uint64_t* results, eh_query_stats* stats) {
   return guarded([&] {
@@ -372,19 +495,27 @@ eh_status eh_query_count_host_csr(eh_context* ctx, const uint32_t* head, uint32_
     t.rows = off[n_head];
     need(t.rows < (1ull << 32), "tries hold fewer than 2^32 rows");
     need(off[0] == 0, "off[0] must be 0");
-    t.head.alloc(n_head ? n_head : 1, s);
-    t.off.alloc(n_head + 1, s);
-    t.vals.alloc(t.rows ? t.rows : 1, s);
-    if (n_head) EH_CUDA(cudaMemcpyAsync(t.head.p, head, n_head * 4, cudaMemcpyHostToDevice, s));
-    EH_CUDA(cudaMemcpyAsync(t.off.p, off, (n_head + 1) * 8, cudaMemcpyHostToDevice, s));
-    if (t.rows) EH_CUDA(cudaMemcpyAsync(t.vals.p, vals, t.rows * 4, cudaMemcpyHostToDevice, s));
-    // the value domain bounds head_index[]: take it from the data, never
-    // from the caller's n_nodes alone
-    const uint32_t mh = n_head ? max_u32(t.head.p, n_head, s) : 0;
-    const uint32_t mv = t.rows ? max_u32(t.vals.p, t.rows, s) : 0;
-    t.n_nodes = (n_head || t.rows) ? std::max(n_nodes, std::max(mh, mv) + 1) : 0;
+    TracePhase all("host_csr.total", s);
+    {
+      TracePhase ph("host_csr.h2d", s);
+      t.head.alloc(n_head ? n_head : 1, s);
+      t.off.alloc(n_head + 1, s);
+      t.vals.alloc(t.rows ? t.rows : 1, s);
+      if (n_head) EH_CUDA(cudaMemcpyAsync(t.head.p, head, n_head * 4, cudaMemcpyHostToDevice, s));
+      EH_CUDA(cudaMemcpyAsync(t.off.p, off, (n_head + 1) * 8, cudaMemcpyHostToDevice, s));
+      if (t.rows) EH_CUDA(cudaMemcpyAsync(t.vals.p, vals, t.rows * 4, cudaMemcpyHostToDevice, s));
+    }
+    {
+      TracePhase ph("host_csr.domain", s);
+      // the value domain bounds head_index[]: take it from the data, never
+      // from the caller's n_nodes alone
+      const uint32_t mh = n_head ? max_u32(t.head.p, n_head, s) : 0;
+      const uint32_t mv = t.rows ? max_u32(t.vals.p, t.rows, s) : 0;
+      t.n_nodes = (n_head || t.rows) ? std::max(n_nodes, std::max(mh, mv) + 1) : 0;
+    }
     trie_build_from_csr(ctx, &t);
     trie_layout(ctx, &t, cfg);
+    TracePhase ph("host_csr.query", s);
     query_count(ctx, &t, query, ecfg, result, stats);
   });
 }

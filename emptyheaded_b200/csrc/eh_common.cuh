@@ -50,8 +50,35 @@ inline int num_sms() {
   return sms;
 }
 
+// ---------------------------------------------------------------- tracing
+// Phase timings on stderr when the environment variable EH_TRACE is set,
+// like the reference's timer::start_clock / stop_clock prints
+// (storage_engine/include/utils/timer.hpp:11-20).  A traced phase
+// synchronises its stream when it begins and ends and reports the wall time
+// between; with EH_TRACE unset it costs one branch.
+bool trace_enabled();
+struct TracePhase {
+  const char* name;
+  cudaStream_t s;
+  double t0 = 0;
+  bool on;
+  TracePhase(const char* n, cudaStream_t st);
+  ~TracePhase() { end(); }
+  void end();  // report now (once)
+  TracePhase(const TracePhase&) = delete;
+  TracePhase& operator=(const TracePhase&) = delete;
+};
+
 // ------------------------------------------------------- device buffers
-// Stream-ordered device allocations (cudaMallocAsync) owned by RAII
+// The engine's stream-ordered memory pool on the current device (one per
+// device, created on first use).  Freed blocks stay in the pool for the next
+// allocation instead of going back to the driver at every synchronisation
+// (the default pool's behaviour): a trie build frees and re-allocates
+// gigabytes between its synchronisations.  eh_context_destroy trims it.
+cudaMemPool_t device_pool();
+void trim_device_pool(int device);
+
+// Stream-ordered device allocations (from device_pool()) owned by RAII
 // handles; a trie and its layouts live in a handful of these.
 template <typename T>
 struct DevBuf {
@@ -76,7 +103,7 @@ struct DevBuf {
     s = stream;
     n = count;
     if (count) {
-      cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T), stream);
+      cudaError_t e = cudaMallocFromPoolAsync((void**)&p, count * sizeof(T), device_pool(), stream);
       if (e != cudaSuccess) {
         p = nullptr;
         n = 0;

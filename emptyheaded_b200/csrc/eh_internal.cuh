@@ -142,6 +142,8 @@ void query_count(eh_context* ctx, const eh_trie* t, int query, const eh_exec_con
 void query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query,
                          const eh_exec_config* cfg, uint64_t* results, eh_query_stats* stats);
 void triangle_annotation(eh_context* ctx, const eh_trie* t, const eh_exec_config* cfg, uint64_t* annot_dev);
+void query_count_select(eh_context* ctx, const eh_trie* t, int query, uint32_t value, const eh_exec_config* cfg,
+                        uint64_t* result, eh_query_stats* stats);
 eh_batch* batch_create(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query,
                        const eh_exec_config* cfg);
 void batch_run(eh_context* ctx, eh_batch* b, uint64_t* results, eh_query_stats* stats);
@@ -150,6 +152,18 @@ void query_count_in_scratch(eh_context* ctx, const eh_trie* t, int query, const 
                             unsigned char* scratch, size_t bytes, uint64_t* result);
 void query_materialize(eh_context* ctx, const eh_trie* t, int query, const eh_exec_config* cfg, int n_cols,
                        uint32_t* a, uint32_t* b, uint32_t* c, uint64_t cap, uint64_t* n_rows);
+
+// dictionary encoding (eh_encode.cu)
+eh_encoding* encoding_build(eh_context* ctx, const void* const* cols, const uint64_t* n_rows, uint32_t n_cols,
+                            int type, int on_device);
+void encoding_encode(eh_context* ctx, const eh_encoding* e, const void* col, uint64_t n, int on_device,
+                     uint32_t* keys);
+void encoding_decode(eh_context* ctx, const eh_encoding* e, const uint32_t* keys, uint64_t n, int on_device,
+                     void* values);
+void encoding_values(eh_context* ctx, const eh_encoding* e, void* values, uint64_t cap);
+uint64_t encoding_size(const eh_encoding* e);
+eh_context* encoding_ctx(const eh_encoding* e);
+void encoding_free(eh_encoding* e);
 
 // learned layout policy (eh_model.cu)
 void model_choose_layouts(eh_context* ctx, const eh_model* m, const eh_trie* t, uint64_t max_bitset_bytes,

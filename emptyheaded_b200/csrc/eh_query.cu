@@ -63,6 +63,7 @@ struct ExecParams {
   uint32_t chunk;
   uint32_t shard_index, shard_count;
   uint32_t long_row;
+  uint32_t s_cap;  // 4-clique: S buffers in global memory of this many words per warp (0: in shared memory)
 };
 
 static ExecParams exec_params(const eh_exec_config* cfg) {
@@ -74,6 +75,7 @@ static ExecParams exec_params(const eh_exec_config* cfg) {
   p.shard_count = (cfg && cfg->shard_count > 1) ? (uint32_t)cfg->shard_count : 1u;
   p.shard_index = (cfg && cfg->shard_count > 1) ? (uint32_t)cfg->shard_index : 0u;
   EH_REQUIRE(p.shard_index < p.shard_count, EH_ERR_INVALID, "shard_index must be below shard_count");
+  p.s_cap = 0;
   p.warps = std::max(1, std::min(p.warps, kMaxWarps));
   p.smem_words = std::max(64, std::min(p.smem_words, 16384)) & ~1;
   return p;
@@ -427,6 +429,9 @@ struct QueryOut {
   uint32_t count_mult;
   const unsigned long long* item_off;  // MODE_MAT: first output row of each item
   uint32_t *ma, *mb, *mc;      // MODE_MAT: output columns
+  const uint32_t* sel;         // 4-clique: bit per node value of a selected partner set, or null
+  uint32_t* gsbuf;             // 4-clique: per-warp S buffers in global memory (sets too large for
+  uint32_t gcap;               //   shared memory), gcap words each; null: S in shared memory
 };
 
 template <int kMode>
@@ -526,13 +531,29 @@ __device__ __forceinline__ uint32_t probe_global_set(const TrieView& t, uint32_t
   return list_contains<false>(t.vals + s0, n, w) ? 1u : 0u;
 }
 
+__device__ __forceinline__ uint32_t sel_bit(const uint32_t* sel, uint32_t x) {
+  return (__ldg(sel + (x >> 5)) >> (x & 31)) & 1u;
+}
+
+// With a selection (sel != null, bit per node value of the partner set
+// {a : (a,v) in Edge}), only 4-cliques whose root a is selected count.  On
+// an oriented relation the row's a is the plan's root: other rows are
+// skipped.  On a symmetric relation the one undirected clique found stands
+// for its 4! orderings, of which 3! start at each member: the hit counts
+// the members that are selected (the host multiplies by 3!).
 template <int P>
 __device__ uint64_t clique_rows(const Staged& st, const TrieView& t, const RevView& r, uint32_t kb, uint32_t ke,
-                                uint32_t* sbuf, uint32_t cap) {
+                                uint32_t* sbuf, uint32_t cap, const uint32_t* sel, uint32_t wb) {
   const uint32_t lane = lane_id();
   const bool up = r.dir != DIR_DOWN;
   uint64_t cnt = 0;
   for (uint32_t k = kb; k < ke; k++) {
+    uint32_t wab = 0;
+    if (sel) {
+      const uint32_t wa = sel_bit(sel, __ldg(t.head + __ldg(r.rev_src + k)));
+      if (r.dir != DIR_SYM && !wa) continue;  // warp-uniform: k is the same on every lane
+      wab = wa + wb;
+    }
     const uint32_t lo = __ldg(r.rev_lo + k), hi = __ldg(r.rev_hi + k);
     // S = N(a)[lo, hi) ∩ N(b), compacted in order
     uint32_t ns = 0;
@@ -558,7 +579,13 @@ __device__ uint64_t clique_rows(const Staged& st, const TrieView& t, const RevVi
       const int32_t hc = __ldg(t.head_index + c);
       if (hc < 0) continue;
       const uint32_t jb = up ? i + 1 : 0, je = up ? ns : i;
-      for (uint32_t j = jb + lane; j < je; j += 32) cnt += probe_global_set(t, (uint32_t)hc, sbuf[j]);
+      if (sel && r.dir == DIR_SYM) {
+        const uint32_t wabc = wab + sel_bit(sel, c);
+        for (uint32_t j = jb + lane; j < je; j += 32)
+          if (probe_global_set(t, (uint32_t)hc, sbuf[j])) cnt += wabc + sel_bit(sel, sbuf[j]);
+      } else {
+        for (uint32_t j = jb + lane; j < je; j += 32) cnt += probe_global_set(t, (uint32_t)hc, sbuf[j]);
+      }
     }
     __syncwarp();
   }
@@ -573,7 +600,10 @@ __global__ void EH_TRI_LAUNCH_BOUNDS clique4_kernel(const TrieView* __restrict__
   const uint32_t lane = lane_id();
   const uint32_t wid = threadIdx.x >> 5;
   uint32_t* sm = smem + (size_t)wid * cap_words;
-  const int half = cap_words / 2;
+  // S after the staged set in the warp's region, or in its global buffer
+  const int half = out.gsbuf ? cap_words : cap_words / 2;
+  uint32_t* sbuf = out.gsbuf ? out.gsbuf + ((size_t)blockIdx.x * (blockDim.x >> 5) + wid) * out.gcap : sm + half;
+  const uint32_t scap = out.gsbuf ? out.gcap : (uint32_t)half;
   unsigned long long acc = 0;
   uint32_t cur_g = 0xffffffffu;
   for (;;) {
@@ -593,14 +623,14 @@ __global__ void EH_TRI_LAUNCH_BOUNDS clique4_kernel(const TrieView* __restrict__
     const RevView r = revs[item.g];
     Staged st;
     const int mode = stage_set(t, item.hb, sm, half, st);
-    uint32_t* sbuf = sm + half;
+    const uint32_t wb = out.sel ? sel_bit(out.sel, t.head[item.hb]) : 0u;
     uint64_t c;
     switch (mode) {
-      case P_SBITS: c = clique_rows<P_SBITS>(st, t, r, item.kb, item.ke, sbuf, half); break;
-      case P_GBITS: c = clique_rows<P_GBITS>(st, t, r, item.kb, item.ke, sbuf, half); break;
-      case P_SLIST: c = clique_rows<P_SLIST>(st, t, r, item.kb, item.ke, sbuf, half); break;
-      case P_GLIST: c = clique_rows<P_GLIST>(st, t, r, item.kb, item.ke, sbuf, half); break;
-      default: c = clique_rows<P_GBLOCK>(st, t, r, item.kb, item.ke, sbuf, half); break;
+      case P_SBITS: c = clique_rows<P_SBITS>(st, t, r, item.kb, item.ke, sbuf, scap, out.sel, wb); break;
+      case P_GBITS: c = clique_rows<P_GBITS>(st, t, r, item.kb, item.ke, sbuf, scap, out.sel, wb); break;
+      case P_SLIST: c = clique_rows<P_SLIST>(st, t, r, item.kb, item.ke, sbuf, scap, out.sel, wb); break;
+      case P_GLIST: c = clique_rows<P_GLIST>(st, t, r, item.kb, item.ke, sbuf, scap, out.sel, wb); break;
+      default: c = clique_rows<P_GBLOCK>(st, t, r, item.kb, item.ke, sbuf, scap, out.sel, wb); break;
     }
     acc += warp_sum(c);
     __syncwarp();
@@ -674,6 +704,8 @@ struct Prepared {
   int query = 0;
   bool annot = false;
   uint32_t plan_launches = 0;
+  const uint32_t* sel = nullptr;  // 4-clique selection bitmap (QueryOut::sel)
+  DevBuf<uint32_t> gs;            // 4-clique global S buffers (ExecParams::s_cap)
 };
 
 static void prepare(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query, ExecParams ep, bool annot,
@@ -742,6 +774,12 @@ static void prepare(eh_context* ctx, const eh_trie* const* tries, uint32_t n, in
   }
   const int per_sm = blocks_per_sm(kfn, P.threads, P.smem);
   P.grid = std::max(1, std::min(num_sms() * per_sm, (int)((total_items + ep.warps - 1) / ep.warps)));
+  if (query == EH_QUERY_CLIQUE4 && ep.s_cap) {
+    // one S buffer per resident warp, at most 2 GiB in all
+    const uint64_t per_block = (uint64_t)ep.warps * ep.s_cap * 4;
+    P.grid = std::max(1, (int)std::min<uint64_t>((uint64_t)P.grid, (2ull << 30) / per_block));
+    P.gs.alloc((size_t)P.grid * ep.warps * ep.s_cap, s);
+  }
   P.ep = ep;
   EH_CUDA(cudaStreamSynchronize(s));  // host staging vectors go out of scope
 }
@@ -755,6 +793,9 @@ static void launch(eh_context* ctx, Prepared& P, unsigned long long* d_total, un
   EH_CUDA(cudaMemsetAsync(P.q.p, 0, 8, s));
   const ExecParams& ep = P.ep;
   QueryOut out{ep.shard_index, ep.shard_count, ep.long_row, d_total, d_annot, d_records, P.q.p, P.q.p + 1};
+  out.sel = P.sel;
+  out.gsbuf = ep.s_cap ? P.gs.p : nullptr;
+  out.gcap = ep.s_cap;
   if (P.query == EH_QUERY_CLIQUE4)
     clique4_kernel<<<P.grid, P.threads, P.smem, s>>>(P.dv.p, P.dr.p, P.items.p, P.n_items, ep.smem_words, out);
   else if (P.annot)
@@ -767,13 +808,27 @@ static void launch(eh_context* ctx, Prepared& P, unsigned long long* d_total, un
 }
 
 // Plan + run + wait; the intersection kernel is timed with events.
+// 4-clique: the warp's shared region holds the staged N(b) and S
+// (S <= the largest set) while that stays within 96 KB a block; beyond, S
+// moves to per-warp global buffers (L2-resident in practice) and the whole
+// region stages N(b).
+static void size_clique_staging(ExecParams& ep, uint32_t max_set) {
+  const int need = 2 * ((int)max_set + 1);
+  if ((size_t)std::max(ep.smem_words, need) * 4 * ep.warps <= 96 * 1024) {
+    if (ep.smem_words < need) ep.smem_words = (need + 1) & ~1;
+  } else {
+    ep.s_cap = max_set + 1;
+  }
+}
+
 static Launch run_plans(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query, ExecParams ep,
                         bool annot, unsigned long long* d_total, unsigned long long* d_annot, float* d_records,
-                        uint32_t* n_items_out, uint64_t* pairs_out) {
+                        uint32_t* n_items_out, uint64_t* pairs_out, const uint32_t* sel = nullptr) {
   cudaStream_t s = ctx->stream;
   Launch L;
   Prepared P;
   prepare(ctx, tries, n, query, ep, annot, P);
+  P.sel = sel;
   L.launches = P.plan_launches;
   *n_items_out = P.n_items;
   *pairs_out = P.pairs;
@@ -819,13 +874,9 @@ void query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t 
                  "4-clique needs a relation that is up-, down-oriented or symmetric");
   ExecParams ep = exec_params(cfg);
   if (query == EH_QUERY_CLIQUE4) {
-    // the warp's region holds the staged set and S (<= the largest set)
     uint32_t mx = 0;
     for (uint32_t g = 0; g < n; g++) mx = std::max(mx, tries[g]->info.max_set);
-    const int need = 2 * ((int)mx + 1);
-    if (ep.smem_words < need) ep.smem_words = (need + 1) & ~1;
-    EH_REQUIRE((size_t)ep.smem_words * 4 * ep.warps <= 200 * 1024, EH_ERR_UNSUPPORTED,
-               "4-clique: largest set too large for the shared-memory staging");
+    size_clique_staging(ep, mx);
   }
   EH_CUDA(cudaEventRecord(ctx->ev0, s));
   DevBuf<unsigned long long> total(n, s);
@@ -907,6 +958,142 @@ void triangle_annotation(eh_context* ctx, const eh_trie* t, const eh_exec_config
   run_plans(ctx, ts, 1, EH_QUERY_TRIANGLE, ep, true, dummy.p, (unsigned long long*)annot_dev, nullptr, &items,
             &pairs);
   EH_CUDA(cudaStreamSynchronize(s));
+}
+
+// ------------------------------------------------------------ selections
+// An equality selection x = v on an attribute with one accessor is answered
+// at the head of its relation (emitHeadContainsSelections,
+// EHGenerator.scala:681-701): the selected bag holds the partners of v with
+// annotation 1 each.  Edge(a,x) in order [x,a] gives
+// partners(v) = {a : (a,v) ∈ Edge}: the head entries whose child set holds
+// v.  One thread per head entry binary-searches v in its sorted list (kept
+// whatever the set's layout).
+//   bits: optional bitmap over node values, set for every partner a;
+//   T:    optional per-head annotation, summed over the partners into
+//         sums[0] and over N(v) ∩ head into sums[1];
+//   sums[2] counts the partners.
+__global__ void select_partners_kernel(TrieView t, uint32_t v, uint32_t* __restrict__ bits,
+                                       const unsigned long long* __restrict__ T,
+                                       unsigned long long* __restrict__ sums) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long s_in = 0, s_out = 0, n_in = 0;
+  for (uint32_t i = tid; i < t.n_head; i += stride) {
+    const uint64_t end = t.off[i + 1];
+    uint64_t lo = t.off[i], hi = end;
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if (__ldg(t.vals + mid) < v) lo = mid + 1; else hi = mid;
+    }
+    if (lo < end && __ldg(t.vals + lo) == v) {
+      n_in++;
+      if (bits) {
+        const uint32_t a = t.head[i];
+        atomicOr(bits + (a >> 5), 1u << (a & 31));
+      }
+      if (T) s_in += T[i];
+    }
+  }
+  if (T && v < t.n_nodes) {
+    const int32_t hv = t.head_index[v];
+    if (hv >= 0)
+      for (uint64_t e = t.off[hv] + tid; e < t.off[hv + 1]; e += stride) {
+        const int32_t hx = __ldg(t.head_index + __ldg(t.vals + e));
+        if (hx >= 0) s_out += T[hx];
+      }
+  }
+  s_in = warp_sum(s_in);
+  s_out = warp_sum(s_out);
+  n_in = warp_sum(n_in);
+  if (lane_id() == 0) {
+    if (s_in) atomicAdd(sums, s_in);
+    if (s_out) atomicAdd(sums + 1, s_out);
+    if (n_in) atomicAdd(sums + 2, n_in);
+  }
+}
+
+// FliqueSelAgg(;z) :- 4-clique(a,b,c,d), Edge(a,x), x=v and
+// BarbellSelAgg(;w) :- triangle(a,b,c), Edge(a,p), Edge(p,x),
+// triangle(x,y,z), p=v (test/graph/travis.py:385-401, 472-487; plans
+// QueryPlannerTest.scala:230-304).
+//  4-clique: the 4-clique plan with its roots restricted to partners(v).
+//  Barbell: bag_1_x_y_z reduces to the scalar sum_{x ∈ N(v)} T(x) and the
+//  root bag to sum_{a ∈ partners(v)} T(a) times it, T the triangle
+//  annotation of the lollipop/barbell bag.
+void query_count_select(eh_context* ctx, const eh_trie* t, int query, uint32_t value, const eh_exec_config* cfg,
+                        uint64_t* result, eh_query_stats* stats) {
+  cudaStream_t s = ctx->stream;
+  EH_REQUIRE(query == EH_QUERY_CLIQUE4_SEL || query == EH_QUERY_BARBELL_SEL, EH_ERR_INVALID,
+             "selection queries are EH_QUERY_CLIQUE4_SEL and EH_QUERY_BARBELL_SEL");
+  EH_REQUIRE(t->ctx == ctx, EH_ERR_INVALID, "trie belongs to another context");
+  ExecParams ep = exec_params(cfg);
+  EH_REQUIRE(ep.shard_count == 1, EH_ERR_UNSUPPORTED, "selection plans run unsharded");
+  const bool clique = query == EH_QUERY_CLIQUE4_SEL;
+  if (clique) {
+    EH_REQUIRE(t->dir != DIR_GENERAL || t->rows == 0, EH_ERR_UNSUPPORTED,
+               "4-clique needs a relation that is up-, down-oriented or symmetric");
+    size_clique_staging(ep, t->info.max_set);
+  }
+  EH_CUDA(cudaEventRecord(ctx->ev0, s));
+  DevBuf<unsigned long long> sums(4, s);  // partner sum, N(v) sum, partners, plan total
+  EH_CUDA(cudaMemsetAsync(sums.p, 0, 32, s));
+  const uint64_t nbits = t->n_nodes ? ((uint64_t)t->n_nodes + 31) / 32 : 1;
+  DevBuf<uint32_t> bits;
+  if (clique) {
+    bits.alloc(nbits, s);
+    EH_CUDA(cudaMemsetAsync(bits.p, 0, nbits * 4, s));
+  }
+  const int sgrid = num_sms() * 8;
+  Launch L;
+  if (t->n_head) {
+    select_partners_kernel<<<sgrid, 256, 0, s>>>(t->view(), value, clique ? bits.p : nullptr, nullptr, sums.p);
+    EH_CHECK_LAUNCH();
+    L.launches++;
+  }
+  // Encoding::value_to_key.at(v) throws for a value in neither column
+  int32_t hv = -1;
+  if (value < t->n_nodes)
+    EH_CUDA(cudaMemcpyAsync(&hv, t->head_index.p + value, 4, cudaMemcpyDeviceToHost, s));
+  unsigned long long h[4] = {0, 0, 0, 0};
+  EH_CUDA(cudaMemcpyAsync(h, sums.p, 32, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaStreamSynchronize(s));
+  EH_REQUIRE(hv >= 0 || h[2] > 0, EH_ERR_INVALID,
+             "selection value " + std::to_string(value) + " is not in the relation");
+  uint32_t items = 0;
+  uint64_t pairs = 0;
+  const eh_trie* ts[1] = {t};
+  uint64_t v = 0;
+  if (h[2] > 0) {  // no partners: the selected bag is empty and so is the join
+    if (clique) {
+      Launch K = run_plans(ctx, ts, 1, EH_QUERY_CLIQUE4, ep, false, sums.p + 3, nullptr, nullptr, &items, &pairs,
+                           bits.p);
+      L.launches += K.launches;
+      L.kernel_ms = K.kernel_ms;
+      EH_CUDA(cudaMemcpyAsync(h, sums.p, 32, cudaMemcpyDeviceToHost, s));
+      EH_CUDA(cudaStreamSynchronize(s));
+      v = h[3];
+      if (t->dir == DIR_SYM) v *= 6ull;  // 3! orderings start at each selected member
+    } else if (hv >= 0) {
+      DevBuf<unsigned long long> T(t->n_head, s), dummy(1, s);
+      EH_CUDA(cudaMemsetAsync(T.p, 0, (size_t)t->n_head * 8, s));
+      EH_CUDA(cudaMemsetAsync(dummy.p, 0, 8, s));
+      EH_CUDA(cudaMemsetAsync(sums.p, 0, 32, s));
+      Launch K = run_plans(ctx, ts, 1, EH_QUERY_TRIANGLE, ep, true, dummy.p, T.p, nullptr, &items, &pairs);
+      select_partners_kernel<<<sgrid, 256, 0, s>>>(t->view(), value, nullptr, T.p, sums.p);
+      EH_CHECK_LAUNCH();
+      L.launches += K.launches + 1;
+      L.kernel_ms = K.kernel_ms;
+      EH_CUDA(cudaMemcpyAsync(h, sums.p, 32, cudaMemcpyDeviceToHost, s));
+      EH_CUDA(cudaStreamSynchronize(s));
+      v = (uint64_t)h[0] * (uint64_t)h[1];
+    }
+  }
+  EH_CUDA(cudaEventRecord(ctx->ev2, s));
+  EH_CUDA(cudaEventSynchronize(ctx->ev2));
+  float qms = 0;
+  EH_CUDA(cudaEventElapsedTime(&qms, ctx->ev0, ctx->ev2));
+  *result = v;
+  fill_stats(stats, qms, L, items, pairs, triangle_algorithmic_bytes(t));
 }
 
 // ------------------------------------------------------------ materialize
@@ -1191,15 +1378,16 @@ eh_batch* batch_create(eh_context* ctx, const eh_trie* const* tries, uint32_t n,
   EH_REQUIRE(query == EH_QUERY_TRIANGLE || query == EH_QUERY_CLIQUE4, EH_ERR_UNSUPPORTED,
              "batches run the triangle or 4-clique plan");
   ExecParams ep = exec_params(cfg);
+  uint32_t mx = 0;
   for (uint32_t g = 0; g < n; g++) {
     EH_REQUIRE(tries[g] && tries[g]->ctx == ctx, EH_ERR_INVALID, "null trie or trie of another context");
     if (query == EH_QUERY_CLIQUE4) {
       EH_REQUIRE(tries[g]->dir != DIR_GENERAL || tries[g]->rows == 0, EH_ERR_UNSUPPORTED,
                  "4-clique needs a relation that is up-, down-oriented or symmetric");
-      const int need = 2 * ((int)tries[g]->info.max_set + 1);
-      if (ep.smem_words < need) ep.smem_words = (need + 1) & ~1;
+      mx = std::max(mx, tries[g]->info.max_set);
     }
   }
+  if (query == EH_QUERY_CLIQUE4) size_clique_staging(ep, mx);
   auto* b = new eh_batch();
   try {
     b->ctx = ctx;

@@ -82,6 +82,11 @@ __global__ void layout_heuristic_kernel(SetSrc src, uint32_t n_sets, int policy,
   }
 }
 
+// Sets with more than kBigSet elements (the head set, hubs of a symmetric
+// relation) are built by grid-wide passes, one set at a time; the
+// warp-per-set kernels below skip them.
+constexpr uint64_t kBigSet = 8192;
+
 // sizes of each set's bitset structure: words (range bitset) or blocks
 __global__ void aux_size_kernel(SetSrc src, uint32_t n_sets, const uint8_t* __restrict__ layout,
                                 SetAux* __restrict__ aux, uint64_t* __restrict__ words, uint64_t* __restrict__ blocks) {
@@ -98,7 +103,7 @@ __global__ void aux_size_kernel(SetSrc src, uint32_t n_sets, const uint8_t* __re
     if (len && l == EH_LAYOUT_RANGE_BITSET) {
       start = p[0] >> 6;
       w = (uint64_t)(p[len - 1] >> 6) - start + 1;
-    } else if (len && l == EH_LAYOUT_BLOCK_BITSET) {
+    } else if (len && l == EH_LAYOUT_BLOCK_BITSET && len <= kBigSet) {
       uint64_t c = 0;
       for (uint64_t j = lane; j < len; j += 32) c += (j == 0 || (p[j] >> 8) != (p[j - 1] >> 8)) ? 1 : 0;
       nb = warp_sum(c);
@@ -131,7 +136,7 @@ __global__ void bitset_fill_kernel(SetSrc src, uint32_t n_sets, const uint8_t* _
     const uint32_t* p;
     uint64_t len;
     src.get(i, p, len);
-    if (!len) continue;
+    if (!len || len > kBigSet) continue;
     const SetAux a = aux[i];
     uint64_t* w = words + a.off;
     uint32_t* r = rank + a.off;
@@ -165,7 +170,7 @@ __global__ void block_fill_kernel(SetSrc src, uint32_t n_sets, const uint8_t* __
     const uint32_t* p;
     uint64_t len;
     src.get(i, p, len);
-    if (!len) continue;
+    if (!len || len > kBigSet) continue;
     const SetAux a = aux[i];
     for (uint32_t j = lane; j < 4 * a.n; j += 32) bwords[4 * a.off + j] = 0;
     __syncwarp();
@@ -186,6 +191,78 @@ __global__ void block_fill_kernel(SetSrc src, uint32_t n_sets, const uint8_t* __
       if (valid) atomicOr((unsigned long long*)&bwords[4 * (a.off + my_block) + ((x >> 6) & 3)], 1ull << (x & 63));
       blk += __popc(ball);
     }
+  }
+}
+
+// ---- grid-wide passes over one big set
+__global__ void big_sets_kernel(SetSrc src, uint32_t n_sets, const uint8_t* __restrict__ layout,
+                                uint32_t* __restrict__ idx, unsigned int* __restrict__ count) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_sets; i += gridDim.x * blockDim.x) {
+    const uint8_t l = layout[i];
+    if (l != EH_LAYOUT_RANGE_BITSET && l != EH_LAYOUT_BLOCK_BITSET) continue;
+    const uint64_t len = i == src.n_head ? src.n_head : src.off[i + 1] - src.off[i];
+    if (len > kBigSet) idx[atomicAdd(count, 1u)] = i;
+  }
+}
+
+// first element of each 256-value block of set i (flag per element)
+__global__ void big_block_flags_kernel(SetSrc src, uint32_t i, uint32_t* __restrict__ flag,
+                                       unsigned long long* __restrict__ nblocks) {
+  const uint32_t* p;
+  uint64_t len;
+  src.get(i, p, len);
+  unsigned long long c = 0;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < len; j += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t f = (j == 0 || (p[j] >> 8) != (p[j - 1] >> 8)) ? 1u : 0u;
+    flag[j] = f;
+    c += f;
+  }
+  c = warp_sum(c);
+  if (lane_id() == 0 && c) atomicAdd(nblocks, c);
+}
+
+__global__ void big_block_count_kernel(const unsigned long long* __restrict__ nblocks, uint32_t i,
+                                       uint64_t* __restrict__ blocks, SetAux* __restrict__ aux) {
+  blocks[i] = *nblocks;
+  aux[i].n = (uint32_t)*nblocks;
+}
+
+__global__ void big_bitset_fill_kernel(SetSrc src, uint32_t i, const SetAux* __restrict__ aux,
+                                       uint64_t* __restrict__ words) {
+  const uint32_t* p;
+  uint64_t len;
+  src.get(i, p, len);
+  const SetAux a = aux[i];
+  uint64_t* w = words + a.off;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < len; j += (uint64_t)gridDim.x * blockDim.x)
+    atomicOr((unsigned long long*)&w[(p[j] >> 6) - a.start], 1ull << (p[j] & 63));
+}
+
+__global__ void big_popc_kernel(const SetAux* __restrict__ aux, uint32_t i, const uint64_t* __restrict__ words,
+                                uint32_t* __restrict__ popc) {
+  const SetAux a = aux[i];
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < a.n; j += gridDim.x * blockDim.x)
+    popc[j] = (uint32_t)__popcll(__ldcg(words + a.off + j));
+}
+
+// pos = exclusive scan of the block-start flags: element j lies in block
+// pos[j] + flag[j] - 1
+__global__ void big_block_fill_kernel(SetSrc src, uint32_t i, const SetAux* __restrict__ aux,
+                                      const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos,
+                                      uint32_t* __restrict__ bid, uint32_t* __restrict__ brank,
+                                      uint64_t* __restrict__ bwords) {
+  const uint32_t* p;
+  uint64_t len;
+  src.get(i, p, len);
+  const SetAux a = aux[i];
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < len; j += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t x = p[j];
+    const uint32_t blk = pos[j] + flag[j] - 1;
+    if (flag[j]) {
+      bid[a.off + blk] = x >> 8;
+      brank[a.off + blk] = (uint32_t)j;
+    }
+    atomicOr((unsigned long long*)&bwords[4 * ((uint64_t)a.off + blk) + ((x >> 6) & 3)], 1ull << (x & 63));
   }
 }
 
@@ -243,6 +320,43 @@ static void build_layout_structs(eh_context* ctx, eh_trie* t) {
   DevBuf<uint64_t> words(n_sets + 1, s), blocks(n_sets + 1, s), tot(2, s);
   aux_size_kernel<<<grid, 256, 0, s>>>(src, n_sets, t->layout.p, t->aux.p, words.p, blocks.p);
   EH_CHECK_LAUNCH();
+  // the big sets, and the block counts of big block-bitset sets
+  std::vector<uint32_t> big;
+  {
+    DevBuf<uint32_t> idx(n_sets, s);
+    DevBuf<unsigned int> cnt(1, s);
+    EH_CUDA(cudaMemsetAsync(cnt.p, 0, 4, s));
+    big_sets_kernel<<<grid, 256, 0, s>>>(src, n_sets, t->layout.p, idx.p, cnt.p);
+    EH_CHECK_LAUNCH();
+    unsigned int nb = 0;
+    EH_CUDA(cudaMemcpyAsync(&nb, cnt.p, 4, cudaMemcpyDeviceToHost, s));
+    EH_CUDA(cudaStreamSynchronize(s));
+    big.resize(nb);
+    if (nb) EH_CUDA(cudaMemcpyAsync(big.data(), idx.p, nb * 4, cudaMemcpyDeviceToHost, s));
+    EH_CUDA(cudaStreamSynchronize(s));
+  }
+  std::vector<uint8_t> big_layout(big.size());
+  std::vector<uint64_t> big_len(big.size());
+  for (size_t k = 0; k < big.size(); k++) {
+    const uint32_t i = big[k];
+    uint64_t o[2] = {0, t->n_head};
+    EH_CUDA(cudaMemcpyAsync(&big_layout[k], t->layout.p + i, 1, cudaMemcpyDeviceToHost, s));
+    if (i < t->n_head) EH_CUDA(cudaMemcpyAsync(o, t->off.p + i, 16, cudaMemcpyDeviceToHost, s));
+    EH_CUDA(cudaStreamSynchronize(s));
+    big_len[k] = o[1] - o[0];
+  }
+  uint64_t big_max = 0;
+  for (uint64_t l : big_len) big_max = std::max(big_max, l);
+  DevBuf<uint32_t> bflag(big_max ? big_max : 1, s), bpos(big_max ? big_max : 1, s), btot(1, s);
+  DevBuf<unsigned long long> bcount(1, s);
+  for (size_t k = 0; k < big.size(); k++) {
+    if (big_layout[k] != EH_LAYOUT_BLOCK_BITSET) continue;
+    EH_CUDA(cudaMemsetAsync(bcount.p, 0, 8, s));
+    big_block_flags_kernel<<<grid, 256, 0, s>>>(src, big[k], bflag.p, bcount.p);
+    EH_CHECK_LAUNCH();
+    big_block_count_kernel<<<1, 1, 0, s>>>(bcount.p, big[k], blocks.p, t->aux.p);
+    EH_CHECK_LAUNCH();
+  }
   exclusive_scan<uint64_t>(words.p, words.p, n_sets, tot.p, s);
   exclusive_scan<uint64_t>(blocks.p, blocks.p, n_sets, tot.p + 1, s);
   aux_offsets_kernel<<<grid, 256, 0, s>>>(n_sets, t->layout.p, words.p, blocks.p, t->aux.p);
@@ -263,6 +377,32 @@ static void build_layout_structs(eh_context* ctx, eh_trie* t) {
     block_fill_kernel<<<grid, 256, 0, s>>>(src, n_sets, t->layout.p, t->aux.p, t->bb_id.p, t->bb_rank.p,
                                            t->bb_words.p);
     EH_CHECK_LAUNCH();
+  }
+  for (size_t k = 0; k < big.size(); k++) {
+    const uint32_t i = big[k];
+    SetAux a{};
+    EH_CUDA(cudaMemcpyAsync(&a, t->aux.p + i, sizeof(SetAux), cudaMemcpyDeviceToHost, s));
+    EH_CUDA(cudaStreamSynchronize(s));
+    if (!a.n) continue;
+    if (big_layout[k] == EH_LAYOUT_RANGE_BITSET) {
+      EH_CUDA(cudaMemsetAsync(t->bs_words.p + a.off, 0, (size_t)a.n * 8, s));
+      big_bitset_fill_kernel<<<grid, 256, 0, s>>>(src, i, t->aux.p, t->bs_words.p);
+      EH_CHECK_LAUNCH();
+      // ranks: exclusive prefix of the words' popcounts
+      DevBuf<uint32_t> popc(a.n, s);
+      big_popc_kernel<<<grid, 256, 0, s>>>(t->aux.p, i, t->bs_words.p, popc.p);
+      EH_CHECK_LAUNCH();
+      exclusive_scan<uint32_t>(popc.p, t->bs_rank.p + a.off, a.n, btot.p, s);
+    } else {
+      EH_CUDA(cudaMemsetAsync(t->bb_words.p + 4 * (uint64_t)a.off, 0, (size_t)a.n * 32, s));
+      EH_CUDA(cudaMemsetAsync(bcount.p, 0, 8, s));
+      big_block_flags_kernel<<<grid, 256, 0, s>>>(src, i, bflag.p, bcount.p);
+      EH_CHECK_LAUNCH();
+      exclusive_scan<uint32_t>(bflag.p, bpos.p, big_len[k], btot.p, s);
+      big_block_fill_kernel<<<grid, 256, 0, s>>>(src, i, t->aux.p, bflag.p, bpos.p, t->bb_id.p, t->bb_rank.p,
+                                                 t->bb_words.p);
+      EH_CHECK_LAUNCH();
+    }
   }
   DevBuf<uint32_t> hist(4, s);
   EH_CUDA(cudaMemsetAsync(hist.p, 0, 16, s));
@@ -302,6 +442,7 @@ void trie_layout(eh_context* ctx, eh_trie* t, const eh_layout_config* cfg) {
              EH_ERR_INVALID, "unknown layout policy");
   EH_REQUIRE(forced == EH_LAYOUT_UINTEGER || forced == EH_LAYOUT_RANGE_BITSET || forced == EH_LAYOUT_BLOCK_BITSET,
              EH_ERR_INVALID, "unknown forced layout");
+  TracePhase ph("layout.choose", s);
   t->layout.alloc(n_sets, s);
   const uint64_t max_words = cfg ? cfg->max_bitset_bytes / 12 : 0;
   layout_heuristic_kernel<<<num_sms() * 4, 256, 0, s>>>(set_src(t), n_sets, policy, forced, max_words,
@@ -311,6 +452,8 @@ void trie_layout(eh_context* ctx, eh_trie* t, const eh_layout_config* cfg) {
     EH_REQUIRE(cfg->model != nullptr, EH_ERR_INVALID, "learned layout policy needs a model");
     model_choose_layouts(ctx, cfg->model, t, cfg->max_bitset_bytes, t->layout.p);
   }
+  ph.end();
+  TracePhase ph_s("layout.structs", s);
   build_layout_structs(ctx, t);
   update_bytes(t);
 }
@@ -318,40 +461,44 @@ void trie_layout(eh_context* ctx, eh_trie* t, const eh_layout_config* cfg) {
 void trie_build_from_csr(eh_context* ctx, eh_trie* t) {
   cudaStream_t s = ctx->stream;
   const int grid = num_sms() * 8;
-  t->head_index.alloc(t->n_nodes ? t->n_nodes : 1, s);
-  EH_CUDA(cudaMemsetAsync(t->head_index.p, 0xff, (size_t)(t->n_nodes ? t->n_nodes : 1) * 4, s));
-  if (t->n_head) {
-    head_index_kernel<<<grid, 256, 0, s>>>(t->head.p, t->n_head, t->head_index.p);
-    EH_CHECK_LAUNCH();
-  }
-  t->wedges.alloc(t->n_head ? t->n_head : 1, s);
-  DevBuf<uint64_t> tot(1, s);
-  if (t->n_head) {
-    wedge_kernel<<<grid, 256, 0, s>>>(t->view(), t->wedges.p);
-    EH_CHECK_LAUNCH();
-    DevBuf<uint64_t> scratch(t->n_head, s);
-    exclusive_scan<uint64_t>(t->wedges.p, scratch.p, t->n_head, tot.p, s);
-    EH_CUDA(cudaMemcpyAsync(&t->total_wedges, tot.p, 8, cudaMemcpyDeviceToHost, s));
-  }
-  EH_CUDA(cudaStreamSynchronize(s));
-  t->info.rows = t->rows;
-  t->info.n_head = t->n_head;
-  t->info.n_nodes = t->n_nodes;
-  // largest set and sum of squared set sizes
-  uint32_t mx = 0;
-  t->sum_sq_deg = 0;
-  if (t->n_head) {
-    DevBuf<unsigned long long> red(2, s);
-    EH_CUDA(cudaMemsetAsync(red.p, 0, 16, s));
-    set_size_stats_kernel<<<grid, 256, 0, s>>>(t->off.p, t->n_head, red.p);
-    EH_CHECK_LAUNCH();
-    unsigned long long h[2];
-    EH_CUDA(cudaMemcpyAsync(h, red.p, 16, cudaMemcpyDeviceToHost, s));
+  {
+    TracePhase ph("build.index+stats", s);
+    t->head_index.alloc(t->n_nodes ? t->n_nodes : 1, s);
+    EH_CUDA(cudaMemsetAsync(t->head_index.p, 0xff, (size_t)(t->n_nodes ? t->n_nodes : 1) * 4, s));
+    if (t->n_head) {
+      head_index_kernel<<<grid, 256, 0, s>>>(t->head.p, t->n_head, t->head_index.p);
+      EH_CHECK_LAUNCH();
+    }
+    t->wedges.alloc(t->n_head ? t->n_head : 1, s);
+    DevBuf<uint64_t> tot(1, s);
+    if (t->n_head) {
+      wedge_kernel<<<grid, 256, 0, s>>>(t->view(), t->wedges.p);
+      EH_CHECK_LAUNCH();
+      DevBuf<uint64_t> scratch(t->n_head, s);
+      exclusive_scan<uint64_t>(t->wedges.p, scratch.p, t->n_head, tot.p, s);
+      EH_CUDA(cudaMemcpyAsync(&t->total_wedges, tot.p, 8, cudaMemcpyDeviceToHost, s));
+    }
     EH_CUDA(cudaStreamSynchronize(s));
-    mx = (uint32_t)h[0];
-    t->sum_sq_deg = h[1];
+    t->info.rows = t->rows;
+    t->info.n_head = t->n_head;
+    t->info.n_nodes = t->n_nodes;
+    // largest set and sum of squared set sizes
+    uint32_t mx = 0;
+    t->sum_sq_deg = 0;
+    if (t->n_head) {
+      DevBuf<unsigned long long> red(2, s);
+      EH_CUDA(cudaMemsetAsync(red.p, 0, 16, s));
+      set_size_stats_kernel<<<grid, 256, 0, s>>>(t->off.p, t->n_head, red.p);
+      EH_CHECK_LAUNCH();
+      unsigned long long h[2];
+      EH_CUDA(cudaMemcpyAsync(h, red.p, 16, cudaMemcpyDeviceToHost, s));
+      EH_CUDA(cudaStreamSynchronize(s));
+      mx = (uint32_t)h[0];
+      t->sum_sq_deg = h[1];
+    }
+    t->info.max_set = mx;
   }
-  t->info.max_set = mx;
+  TracePhase ph("build.reverse", s);
   trie_build_reverse(ctx, t);
 }
 
@@ -366,6 +513,7 @@ void trie_build(eh_context* ctx, const uint32_t* c0, const uint32_t* c1, uint64_
   uint64_t r = 0;
   t->n_nodes = n ? std::max(m0, m1) + 1 : 0;
   if (n) {
+    TracePhase ph("build.sort+csr", s);
     DevBuf<uint64_t> keys(n, s), tmp(n, s);
     pack_rows_kernel<<<grid, 256, 0, s>>>(c0, c1, n, b, keys.p);
     EH_CHECK_LAUNCH();
@@ -506,6 +654,7 @@ void trie_build_reverse(eh_context* ctx, eh_trie* t) {
   }
   EH_REQUIRE(t->rows < (1ull << 32), EH_ERR_UNSUPPORTED, "tries with 2^32 rows or more are not supported");
   DevBuf<uint32_t> seg(t->rows, s);
+  TracePhase ph_dir("reverse.direction", s);
   seg_kernel<<<grid, 256, 0, s>>>(t->off.p, t->n_head, seg.p);
   EH_CHECK_LAUNCH();
   // direction: up / down from one cheap pass; the mirror search only when
@@ -531,6 +680,7 @@ void trie_build_reverse(eh_context* ctx, eh_trie* t) {
     // triangle once, times 3!) only without self-loops
     t->dir = (c[2] == 0 && c[3] == 0) ? DIR_SYM : DIR_GENERAL;
   }
+  ph_dir.end();
   // group the rows a->b the plans read by b (stable: row order within b)
   const int bh = bits_for(t->n_head);
   const uint64_t sentinel = (1ull << bh) - 1;  // above every head position
@@ -538,9 +688,14 @@ void trie_build_reverse(eh_context* ctx, eh_trie* t) {
   DevBuf<uint32_t> rowid(t->rows, s), vtmp(t->rows, s);
   DevBuf<uint32_t> per(t->n_head + 1, s);
   EH_CUDA(cudaMemsetAsync(per.p, 0, (t->n_head + 1) * 4, s));
+  TracePhase ph_key("reverse.keys", s);
   rev_key_kernel<<<grid, 256, 0, s>>>(t->view(), seg.p, t->dir, sentinel, keys.p, rowid.p, per.p);
   EH_CHECK_LAUNCH();
+  ph_key.end();
+  TracePhase ph_sort("reverse.sort", s);
   radix_sort_kv(keys.p, ktmp.p, rowid.p, vtmp.p, t->rows, bh, s);
+  ph_sort.end();
+  TracePhase ph_fill("reverse.offsets+fill", s);
   {
     DevBuf<uint64_t> per64(t->n_head + 1, s);
     widen_u32_kernel<<<grid, 256, 0, s>>>(per.p, t->n_head + 1, per64.p);

@@ -52,7 +52,10 @@ enum {
   EH_QUERY_TRIANGLE = 0, /* TriangleAgg(;z) :- Edge(a,b),Edge(b,c),Edge(a,c),z:long<-[COUNT(*)] */
   EH_QUERY_CLIQUE4 = 1,  /* FliqueAgg(;z) :- 4-clique, COUNT(*) */
   EH_QUERY_LOLLIPOP = 2, /* LollipopAgg(;z) :- triangle + Edge(a,x), COUNT(*) (2 bags) */
-  EH_QUERY_BARBELL = 3   /* BarbellAgg(;w) :- two triangles + Edge(a,x), COUNT(*) (2 bags) */
+  EH_QUERY_BARBELL = 3,  /* BarbellAgg(;w) :- two triangles + Edge(a,x), COUNT(*) (2 bags) */
+  /* equality-selection plans, run by eh_query_count_select only */
+  EH_QUERY_CLIQUE4_SEL = 4, /* FliqueSelAgg(;z) :- 4-clique(a,b,c,d),Edge(a,x),x=value */
+  EH_QUERY_BARBELL_SEL = 5  /* BarbellSelAgg(;w) :- triangle(a,b,c),Edge(a,p),Edge(p,x),triangle(x,y,z),p=value */
 };
 
 typedef struct eh_context eh_context;
@@ -93,6 +96,34 @@ eh_status eh_graph_chunglu(eh_context* ctx, uint64_t seed, uint32_t n, uint64_t 
  * order-preserving dictionary encoding is the identity on these ids. */
 eh_status eh_graph_preprocess(eh_context* ctx, const uint32_t* u, const uint32_t* v, uint64_t m, int symmetric,
                               uint32_t** src, uint32_t** dst, uint64_t* rows, uint32_t* nodes);
+
+/* ------------------------------------------------------ dictionary encoding
+ * Replaces Encoding<T> (storage_engine/include/Encoding.hpp,
+ * storage_engine/src/Encoding.cpp:21-48) as the loader uses it
+ * (query_compiler/.../codegen/create/createDB.scala:242-270).  Value types
+ * are the reference's numeric instantiations: uint32_t, int, long, float
+ * (strings stay with the host).  Keys are assigned in ascending value order
+ * over the distinct values of every column given to eh_encoding_build
+ * (Encoding::build over a std::set), so key 0 is the smallest value.
+ * Columns and outputs are device pointers when on_device != 0, else host
+ * pointers.  Encoding a value the dictionary lacks is EH_ERR_INVALID (the
+ * reference's value_to_key.at throws); so is a NaN float. */
+enum { EH_VALUE_UINT32 = 0, EH_VALUE_INT32 = 1, EH_VALUE_INT64 = 2, EH_VALUE_FLOAT32 = 3 };
+typedef struct eh_encoding eh_encoding;
+/* Encoding<T>::build over all values of n_cols columns */
+eh_status eh_encoding_build(eh_context* ctx, const void* const* cols, const uint64_t* n_rows, uint32_t n_cols,
+                            int value_type, int on_device, eh_encoding** out);
+/* Encoding<T>::encode_column: keys[i] = value_to_key.at(col[i]) */
+eh_status eh_encoding_encode(eh_context* ctx, const eh_encoding* enc, const void* col, uint64_t n, int on_device,
+                             uint32_t* keys);
+/* key_to_value: values[i] = key_to_value[keys[i]] (a key out of range is EH_ERR_INVALID) */
+eh_status eh_encoding_decode(eh_context* ctx, const eh_encoding* enc, const uint32_t* keys, uint64_t n,
+                             int on_device, void* values);
+/* num_distinct, and the key_to_value table (first cap entries) on the host,
+ * the values Encoding::to_binary writes (Encoding.cpp:114-124) */
+eh_status eh_encoding_size(const eh_encoding* enc, uint64_t* n_distinct);
+eh_status eh_encoding_values(eh_context* ctx, const eh_encoding* enc, void* values, uint64_t cap);
+eh_status eh_encoding_free(eh_encoding* enc);
 
 /* ------------------------------------------------------------------ trie */
 typedef struct {
@@ -207,6 +238,21 @@ eh_status eh_query_count(eh_context* ctx, const eh_trie* trie, int query, const 
  * GPU work touching the array concurrently would race. */
 eh_status eh_query_count_noalloc(eh_context* ctx, const eh_trie* trie, int query, const eh_exec_config* cfg,
                                  uint64_t* result);
+
+/* Equality-selection COUNT plans (test/graph/travis.py:385-401, 472-487;
+ * plans query_compiler/src/test/scala/QueryPlannerTest.scala:230-304).
+ * Replaces the generated selection bags: emitSelectionValues /
+ * emitHeadContainsSelections (EHGenerator.scala:657-701) answer the selected
+ * attribute at the head with get_next_block(value_to_key.at(value))
+ * (TrieIterator.cpp:72-78), and the bag of the selected value's partners
+ * joins the 4-clique or triangle bags.  query: EH_QUERY_CLIQUE4_SEL or
+ * EH_QUERY_BARBELL_SEL; value: the selection literal, a value of the
+ * relation's columns.  A value in neither column is EH_ERR_INVALID (the
+ * reference's value_to_key.at throws).  A value without partners counts 0
+ * (the reference's generated code reads a null or out-of-range block
+ * there, TrieBlock.hpp:86-111).  Count modulo 2^64 as for eh_query_count. */
+eh_status eh_query_count_select(eh_context* ctx, const eh_trie* trie, int query, uint32_t value,
+                                const eh_exec_config* cfg, uint64_t* result, eh_query_stats* stats);
 
 /* Materialized output of the triangle plan, rows sorted lexicographically
  * (the order Trie::foreach, storage_engine/src/Trie.cpp:130-160, walks the

@@ -433,6 +433,81 @@ uint64_t eho_clique4(const uint32_t* head, uint32_t nh, const uint64_t* off, con
   return t;
 }
 
+/* ---- equality selections (EHGenerator.scala:657-701) ----
+ * A selected attribute x = v with one accessor is answered at the head of
+ * its relation: get_next_block(key(v)) (ParTrieIterator::get_next_block,
+ * TrieIterator.cpp:72-78) leaves the set of partners of v.  For Edge(a,x)
+ * in order [x,a] that set is {a : (a,v) ∈ Edge}: the head entries whose
+ * child set holds v.  mask[i] = 1 for those entries. */
+static void select_in(const uint32_t* head, uint32_t nh, const uint64_t* off, const uint32_t* vals, uint32_t v,
+                      uint8_t* mask) {
+  (void)head;
+  for (uint32_t i = 0; i < nh; i++) {
+    uint64_t lo = off[i], hi = off[i + 1];
+    while (lo < hi) {
+      const uint64_t mid = lo + (hi - lo) / 2;
+      if (vals[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    mask[i] = (lo < off[i + 1] && vals[lo] == v) ? 1 : 0;
+  }
+}
+
+/* FliqueSelAgg(;z) :- 4-clique(a,b,c,d), Edge(a,x), x=v, COUNT(*)
+ * (travis.py:385-401; plan QueryPlannerTest.scala:230-259): bag_1(a;z)
+ * holds z(a) = 1 for every a with (a,v) ∈ Edge, and the 4-clique root bag
+ * joins it at a, so only roots a of that set count. */
+uint64_t eho_clique4_sel(const uint32_t* head, uint32_t nh, const uint64_t* off, const uint32_t* vals, uint32_t v) {
+  uint8_t* mask = (uint8_t*)malloc(nh ? nh : 1);
+  select_in(head, nh, off, vals, v, mask);
+  /* the FliqueAgg loop nest of eho_clique4, over the selected roots only */
+  uint64_t total = 0;
+  uint32_t* s = NULL;
+  uint64_t cap = 0;
+  for (uint32_t ia = 0; ia < nh; ia++) {
+    if (!mask[ia]) continue;
+    const uint32_t* na = vals + off[ia];
+    const uint64_t da = off[ia + 1] - off[ia];
+    if (da > cap) { free(s); cap = da; s = (uint32_t*)malloc(cap * sizeof(uint32_t)); }
+    for (uint64_t j = 0; j < da; j++) {
+      int64_t ib = head_find(head, nh, na[j]);
+      if (ib < 0) continue;
+      const uint64_t ns = eho_intersect(vals + off[ib], off[ib + 1] - off[ib], na, da, s);
+      for (uint64_t q = 0; q < ns; q++) {
+        int64_t ic = head_find(head, nh, s[q]);
+        if (ic < 0) continue;
+        total += eho_intersect(vals + off[ic], off[ic + 1] - off[ic], s, ns, NULL);
+      }
+    }
+  }
+  free(s);
+  free(mask);
+  return total;
+}
+
+/* BarbellSelAgg(;w) :- triangle(a,b,c), Edge(a,p), Edge(p,x),
+ * triangle(x,y,z), p=v, COUNT(*) (travis.py:472-487; plan
+ * QueryPlannerTest.scala:262-304): bag_1_p_a marks {a : (a,v) ∈ Edge},
+ * bag_2_p_x marks N(v); the x,y,z bag reduces to the scalar
+ * sum_{x ∈ N(v)} T(x) and the root bag to sum_{a : (a,v)} T(a) times it. */
+uint64_t eho_barbell_sel(const uint32_t* head, uint32_t nh, const uint64_t* off, const uint32_t* vals, uint32_t v) {
+  uint64_t* T = (uint64_t*)malloc((nh ? nh : 1) * sizeof(uint64_t));
+  uint8_t* mask = (uint8_t*)malloc(nh ? nh : 1);
+  eho_triangle_per_vertex(head, nh, off, vals, T);
+  select_in(head, nh, off, vals, v, mask);
+  uint64_t s_in = 0, s_out = 0;
+  for (uint32_t i = 0; i < nh; i++)
+    if (mask[i]) s_in += T[i];
+  const int64_t ip = head_find(head, nh, v);
+  if (ip >= 0)
+    for (uint64_t j = off[ip]; j < off[ip + 1]; j++) {
+      const int64_t ix = head_find(head, nh, vals[j]);
+      if (ix >= 0) s_out += T[ix];
+    }
+  free(mask);
+  free(T);
+  return s_in * s_out;
+}
+
 /* bag_1(a;z) of lollipop/barbell (QueryPlannerTest.scala:199-212):
  * T(a) = sum over b ∈ N(a) ∩ head of |N(a) ∩ N(b)|, annotated per a
  * (TrieBuilder::set_annotation, TrieBuilder.cpp:428-446). */

@@ -72,6 +72,11 @@ void eho_triangle_annot(const uint32_t* head, uint32_t nh, const uint64_t* off, 
                         uint64_t* T);
 uint64_t eho_lollipop(const uint32_t* head, uint32_t nh, const uint64_t* off, const uint32_t* vals);
 uint64_t eho_barbell(const uint32_t* head, uint32_t nh, const uint64_t* off, const uint32_t* vals);
+/* equality-selection variants (travis.py:385-401, 472-487): only roots a
+ * with (a,v) in the relation count; the barbell's second triangle starts
+ * in N(v) */
+uint64_t eho_clique4_sel(const uint32_t* head, uint32_t nh, const uint64_t* off, const uint32_t* vals, uint32_t v);
+uint64_t eho_barbell_sel(const uint32_t* head, uint32_t nh, const uint64_t* off, const uint32_t* vals, uint32_t v);
 /* per-head triangle contribution sum_{b in N(a)} |N(a) ∩ N(b)| */
 void eho_triangle_per_vertex(const uint32_t* head, uint32_t nh, const uint64_t* off, const uint32_t* vals,
                              uint64_t* per);

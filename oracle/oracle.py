@@ -73,6 +73,10 @@ def lib():
             f.restype = ctypes.c_uint64
             f.argtypes = [_u32p, ctypes.c_uint32, _u64p, _u32p]
         L.eho_triangle_per_vertex.argtypes = [_u32p, ctypes.c_uint32, _u64p, _u32p, _u64p]
+        for q in ("eho_clique4_sel", "eho_barbell_sel"):
+            f = getattr(L, q)
+            f.restype = ctypes.c_uint64
+            f.argtypes = [_u32p, ctypes.c_uint32, _u64p, _u32p, ctypes.c_uint32]
         L.eho_triangle_list.restype = ctypes.c_uint64
         L.eho_triangle_list.argtypes = [_u32p, ctypes.c_uint32, _u64p, _u32p, _u32p, _u32p, _u32p, ctypes.c_uint64]
         L.eho_triangle_annot.argtypes = [_u32p, ctypes.c_uint32, _u64p, _u32p, _u64p]
@@ -174,6 +178,14 @@ class Trie:
     def barbell(self):
         return int(lib().eho_barbell(*self._args()))
 
+    def clique4_sel(self, v):
+        """FliqueSelAgg: 4-cliques (a,b,c,d) with (a,v) in the relation."""
+        return int(lib().eho_clique4_sel(*self._args(), v))
+
+    def barbell_sel(self, v):
+        """BarbellSelAgg: barbells joined through the selected vertex p = v."""
+        return int(lib().eho_barbell_sel(*self._args(), v))
+
     def triangle_tuples(self):
         """Triangle(a,b,c) rows in (a,b,c) order, as an (n, 3) uint32 array."""
         L = lib()
@@ -267,20 +279,67 @@ def ref_available():
     return os.path.exists(REF_BIN)
 
 
-def ref_query(mode, edges_path, repeats=1, threads=None, timeout=None):
-    """Run the reference engine on an edge file; returns its JSON dict."""
+def ref_query(mode, edges_path, repeats=1, threads=None, timeout=None, value=None):
+    """Run the reference engine on an edge file; returns its JSON dict.
+    `value` is the selection literal of the *_sel modes."""
     env = dict(os.environ)
     if threads:
         env["EH_REF_THREADS"] = str(threads)
+    args = [REF_BIN, mode, edges_path, str(repeats)] + ([] if value is None else [str(int(value))])
     with tempfile.TemporaryDirectory() as td:
         env["TMPDIR"] = td
-        out = subprocess.run([REF_BIN, mode, edges_path, str(repeats)], env=env, capture_output=True,
-                             text=True, timeout=timeout, check=True).stdout
+        out = subprocess.run(args, env=env, capture_output=True, text=True, timeout=timeout, check=True).stdout
     return json.loads(out.strip().splitlines()[-1])
 
 
-def ref_query_edges(mode, src, dst, repeats=1, threads=None, timeout=None):
+def ref_query_edges(mode, src, dst, repeats=1, threads=None, timeout=None, value=None):
     with tempfile.TemporaryDirectory() as td:
         p = os.path.join(td, "edges.bin")
         write_edge_file(p, src, dst)
-        return ref_query(mode, p, repeats, threads, timeout)
+        return ref_query(mode, p, repeats, threads, timeout, value)
+
+
+# ---------------------------------------------------- dictionary encoding
+VALUE_TYPES = {"uint32": (0, np.uint32), "int32": (1, np.int32), "int64": (2, np.int64), "float32": (3, np.float32)}
+
+
+def encoding(cols, value_type):
+    """Encoding<T>::build over every column, then encode_column per column
+    (storage_engine/src/Encoding.cpp:21-48): keys in ascending value order
+    over the distinct values (std::set order; -0.0 and +0.0 are one value).
+    Returns (key_to_value, [keys per column])."""
+    dt = VALUE_TYPES[value_type][1]
+    cols = [np.ascontiguousarray(c, dt) for c in cols]
+    allv = np.concatenate(cols) if cols else np.zeros(0, dt)
+    if value_type == "float32":
+        allv = np.where(allv == 0, np.float32(0), allv).astype(dt)
+        assert not np.isnan(allv).any()
+    values = np.unique(allv)
+    keys = [np.searchsorted(values, np.where(c == 0, 0, c).astype(dt) if value_type == "float32" else c)
+            .astype(np.uint32) for c in cols]
+    return values, keys
+
+
+def ref_encoding(cols, value_type):
+    """The reference's own Encoding<T> (oracle/_ref/eh_ref encode)."""
+    code, dt = VALUE_TYPES[value_type]
+    cols = [np.ascontiguousarray(c, dt) for c in cols]
+    with tempfile.TemporaryDirectory() as td:
+        inp, outp = os.path.join(td, "cols.bin"), os.path.join(td, "out.bin")
+        with open(inp, "wb") as f:
+            f.write(np.array([code, len(cols)], np.uint32).tobytes())
+            for c in cols:
+                f.write(np.uint64(len(c)).tobytes())
+                f.write(c.tobytes())
+        subprocess.run([REF_BIN, "encode", inp, outp], check=True, capture_output=True,
+                       env=dict(os.environ, TMPDIR=td))
+        buf = open(outp, "rb").read()
+    nd = int(np.frombuffer(buf, np.uint32, 1, 0)[0])
+    pos = 4
+    values = np.frombuffer(buf, dt, nd, pos).copy()
+    pos += nd * np.dtype(dt).itemsize
+    keys = []
+    for c in cols:
+        keys.append(np.frombuffer(buf, np.uint32, len(c), pos).copy())
+        pos += 4 * len(c)
+    return values, keys

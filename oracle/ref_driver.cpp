@@ -19,8 +19,12 @@
  *
  * Modes (all print one JSON line on stdout):
  *   eh_ref triangle|clique4|lollipop|barbell <edges> [repeats]
+ *   eh_ref clique4_sel|barbell_sel <edges> <repeats> <value>
+ *                                         the travis.py selection queries
+ *                                         (x = value, p = value)
  *   eh_ref trie_dump <edges> <out.bin>      dump the reference trie
  *   eh_ref setops <pairs.bin> <out.bin>     per-pair ops::set_intersect
+ *   eh_ref encode <cols.bin> <out.bin>      Encoding<T> build + encode_column
  * <edges> is a .tsv (two uint32 columns) or an edge file written by the
  * project's graph generator ("EHEDGE01" header, u64 n, u32 src[n], u32 dst[n]).
  *
@@ -41,6 +45,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -90,9 +95,11 @@ static bool read_edges(const std::string& path, std::vector<uint32_t>& s, std::v
   return true;
 }
 
-/* order-preserving dictionary encoding over both columns */
-static uint32_t encode(std::vector<uint32_t>& s, std::vector<uint32_t>& d) {
-  std::vector<uint32_t> vals(s);
+/* order-preserving dictionary encoding over both columns; key_to_value
+ * receives the distinct values in key order */
+static uint32_t encode(std::vector<uint32_t>& s, std::vector<uint32_t>& d, std::vector<uint32_t>& key_to_value) {
+  std::vector<uint32_t>& vals = key_to_value;
+  vals = s;
   vals.insert(vals.end(), d.begin(), d.end());
   std::sort(vals.begin(), vals.end());
   vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
@@ -102,6 +109,16 @@ static uint32_t encode(std::vector<uint32_t>& s, std::vector<uint32_t>& d) {
       for (auto& x : *col) x = (uint32_t)(std::lower_bound(vals.begin(), vals.end(), x) - vals.begin());
   }
   return (uint32_t)vals.size();
+}
+
+/* Encoding::value_to_key.at(v) (EHGenerator.scala:657-667): the key of a
+ * selection literal; a value absent from the relation is an error there
+ * (std::map::at throws) and here */
+static bool value_to_key(const std::vector<uint32_t>& key_to_value, uint32_t v, uint32_t* key) {
+  auto it = std::lower_bound(key_to_value.begin(), key_to_value.end(), v);
+  if (it == key_to_value.end() || *it != v) return false;
+  *key = (uint32_t)(it - key_to_value.begin());
+  return true;
 }
 
 static Trie<void*, MB>* build_edge_trie(const std::string& dir, std::vector<uint32_t>& s,
@@ -330,6 +347,214 @@ static long bag_barbell_root(Trie<void*, MB>* Trie_Edge_0_1, Trie<long, MB>* Tri
 }
 
 /* ------------------------------------------------------------ dumps */
+/* ------------------------------------------------------- selection bags
+ * A bag whose first attribute carries an equality selection and one
+ * accessor is answered at the head (emitHeadContainsSelections,
+ * EHGenerator.scala:681-701): get_next_block(selection) moves the
+ * iterator's head to the selected value's child set, and the remaining
+ * attribute is materialised with its annotation (SUM over the selected
+ * attribute of 1, i.e. 1 per partner).
+ *   bag_1_x_a_FliqueSelAgg(a;z) :- Edge(a,x), x=v   (order [x,a], trie Edge_1_0)
+ *   bag_1_p_a_BarbellSelAgg(a;w) :- Edge(a,p), p=v  (order [p,a], trie Edge_1_0)
+ *   bag_2_p_x_BarbellSelAgg(x;w) :- Edge(p,x), p=v  (order [p,x], trie Edge_0_1)
+ * (QueryPlannerTest.scala:230-304).  Returns null when v heads no set: the
+ * generated code would dereference a null block there.  A v above the
+ * head's last value is treated the same way: on a dense head,
+ * TrieBlock::get_next_block indexes the next-level array by value
+ * (TrieBlock.hpp:88-95) and would read past its end. */
+static Trie<long, MB>* bag_selected_partners(Trie<void*, MB>* Trie_Edge, uint32_t selection_0, const std::string& out) {
+  mkdir(out.c_str(), 0755);
+  mkdir((out + "/ram").c_str(), 0755);
+  const Set<hybrid>* head_set = Trie_Edge->getHead()->get_const_set();
+  if (head_set->cardinality == 0 || selection_0 > head_set->range) return nullptr;
+  ParTrieIterator<void*, MB> Iterators_Edge(Trie_Edge);
+  Iterators_Edge.get_next_block(selection_0);
+  if (Iterators_Edge.head == nullptr) return nullptr;
+  Trie<long, MB>* Trie_bag = new Trie<long, MB>(out, 1, true);
+  {
+    ParTrieBuilder<long, MB> Builders(Trie_bag, 2);
+    const size_t count_a = Builders.build_set(Iterators_Edge.head);
+    Builders.allocate_annotation();
+    Builders.par_foreach_builder([&](const size_t tid, const uint32_t a_i, const uint32_t a_d) {
+      TrieBuilder<long, MB>* Builder = Builders.builders.at(tid);
+      Builder->set_annotation((long)1, a_i, a_d);
+    });
+    Builders.trie->num_rows = count_a;
+  }
+  return Trie_bag;
+}
+
+/* FliqueSelAgg(;z) root bag, order [a,b,c,d]: the FliqueAgg loop nest with
+ * bag_1(a;z) joined at a (its head in a's intersection, z(a) multiplied in) */
+static long bag_clique4_sel_root(Trie<void*, MB>* Trie_Edge_0_1, Trie<long, MB>* Trie_bag_1, const std::string& out) {
+  typedef const TrieBlock<hybrid, MB>* TB;
+  Trie<long, MB>* Trie_FliqueSelAgg_ = new Trie<long, MB>(out, 0, true);
+  long result;
+  {
+    ParTrieBuilder<long, MB> Builders(Trie_FliqueSelAgg_, 4);
+    ParTrieIterator<void*, MB> Iterators_Edge_c_d(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_b_c(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_b_d(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_c(Trie_Edge_0_1);
+    ParTrieIterator<long, MB> Iterators_bag_1_a(Trie_bag_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_d(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_b(Trie_Edge_0_1);
+    std::vector<TB> a_sets;
+    a_sets.push_back(Iterators_Edge_a_c.head);
+    a_sets.push_back(Iterators_bag_1_a.head);
+    a_sets.push_back(Iterators_Edge_a_d.head);
+    a_sets.push_back(Iterators_Edge_a_b.head);
+    const size_t count_a = Builders.build_aggregated_set(&a_sets);
+    (void)count_a;
+    par::reducer<long> annotation_a(0, [&](long a, long b) { return a + b; });
+    Builders.par_foreach_aggregate([&](const size_t tid, const uint32_t a_d) {
+      TrieBuilder<long, MB>* Builder = Builders.builders.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_c_d = Iterators_Edge_c_d.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_b_c = Iterators_Edge_b_c.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_b_d = Iterators_Edge_b_d.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_c = Iterators_Edge_a_c.iterators.at(tid);
+      TrieIterator<long, MB>* Iterator_bag_1_a = Iterators_bag_1_a.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_d = Iterators_Edge_a_d.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_b = Iterators_Edge_a_b.iterators.at(tid);
+      Iterator_Edge_a_c->get_next_block(0, a_d);
+      Iterator_Edge_a_d->get_next_block(0, a_d);
+      Iterator_Edge_a_b->get_next_block(0, a_d);
+      std::vector<TB> b_sets;
+      b_sets.push_back(Iterator_Edge_b_c->get_block(0));
+      b_sets.push_back(Iterator_Edge_b_d->get_block(0));
+      b_sets.push_back(Iterator_Edge_a_b->get_block(1));
+      const size_t count_b = Builder->build_aggregated_set(&b_sets);
+      (void)count_b;
+      long annotation_b = (long)0;
+      Builder->foreach_aggregate([&](const uint32_t b_d) {
+        Iterator_Edge_b_c->get_next_block(0, b_d);
+        Iterator_Edge_b_d->get_next_block(0, b_d);
+        std::vector<TB> c_sets;
+        c_sets.push_back(Iterator_Edge_c_d->get_block(0));
+        c_sets.push_back(Iterator_Edge_b_c->get_block(1));
+        c_sets.push_back(Iterator_Edge_a_c->get_block(1));
+        const size_t count_c = Builder->build_aggregated_set(&c_sets);
+        (void)count_c;
+        long annotation_c = (long)0;
+        Builder->foreach_aggregate([&](const uint32_t c_d) {
+          Iterator_Edge_c_d->get_next_block(0, c_d);
+          std::vector<TB> d_sets;
+          d_sets.push_back(Iterator_Edge_c_d->get_block(1));
+          d_sets.push_back(Iterator_Edge_b_d->get_block(1));
+          d_sets.push_back(Iterator_Edge_a_d->get_block(1));
+          const size_t count_d = Builder->build_aggregated_set(&d_sets);
+          const long intermediate_d = (long)1 * (count_d * 1);
+          annotation_c += intermediate_d;
+        });
+        annotation_b += annotation_c;
+      });
+      const long intermediate_a = (long)1 * Iterator_bag_1_a->get_annotation(0, a_d) * annotation_b;
+      annotation_a.update(tid, intermediate_a);
+    });
+    Builders.trie->annotation = annotation_a.evaluate(0);
+    result = Builders.trie->annotation;
+  }
+  delete Trie_FliqueSelAgg_;
+  return result;
+}
+
+/* bag_1_x_y_z_BarbellSelAgg(;w) :- Edge(y,z),Edge(x,z),Edge(x,y),bag_2(x;w)
+ * (order [x,y,z]): a scalar, passed into the root bag */
+static long bag_triangle_sel_scalar(Trie<void*, MB>* Trie_Edge_0_1, Trie<long, MB>* Trie_bag_2, const std::string& out) {
+  typedef const TrieBlock<hybrid, MB>* TB;
+  Trie<long, MB>* Trie_bag_xyz = new Trie<long, MB>(out, 0, true);
+  long result;
+  {
+    ParTrieBuilder<long, MB> Builders(Trie_bag_xyz, 3);
+    ParTrieIterator<void*, MB> Iterators_Edge_y_z(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_x_z(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_x_y(Trie_Edge_0_1);
+    ParTrieIterator<long, MB> Iterators_bag_2_x(Trie_bag_2);
+    std::vector<TB> x_sets;
+    x_sets.push_back(Iterators_Edge_x_z.head);
+    x_sets.push_back(Iterators_Edge_x_y.head);
+    x_sets.push_back(Iterators_bag_2_x.head);
+    const size_t count_x = Builders.build_aggregated_set(&x_sets);
+    (void)count_x;
+    par::reducer<long> annotation_x(0, [&](long a, long b) { return a + b; });
+    Builders.par_foreach_aggregate([&](const size_t tid, const uint32_t x_d) {
+      TrieBuilder<long, MB>* Builder = Builders.builders.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_y_z = Iterators_Edge_y_z.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_x_z = Iterators_Edge_x_z.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_x_y = Iterators_Edge_x_y.iterators.at(tid);
+      TrieIterator<long, MB>* Iterator_bag_2_x = Iterators_bag_2_x.iterators.at(tid);
+      Iterator_Edge_x_z->get_next_block(0, x_d);
+      Iterator_Edge_x_y->get_next_block(0, x_d);
+      const size_t count_y =
+          Builder->build_aggregated_set(Iterator_Edge_y_z->get_block(0), Iterator_Edge_x_y->get_block(1));
+      (void)count_y;
+      long annotation_y = (long)0;
+      Builder->foreach_aggregate([&](const uint32_t y_d) {
+        Iterator_Edge_y_z->get_next_block(0, y_d);
+        const size_t count_z =
+            Builder->build_aggregated_set(Iterator_Edge_y_z->get_block(1), Iterator_Edge_x_z->get_block(1));
+        const long intermediate_z = (long)1 * (count_z * 1);
+        annotation_y += intermediate_z;
+      });
+      const long intermediate_x = (long)1 * Iterator_bag_2_x->get_annotation(0, x_d) * annotation_y;
+      annotation_x.update(tid, intermediate_x);
+    });
+    Builders.trie->annotation = annotation_x.evaluate(0);
+    result = Builders.trie->annotation;
+  }
+  delete Trie_bag_xyz;
+  return result;
+}
+
+/* BarbellSelAgg(;w) root bag, order [a,b,c]: Edge(b,c), scalar bag,
+ * bag_1_p_a(a;w), Edge(a,c), Edge(a,b) */
+static long bag_barbell_sel_root(Trie<void*, MB>* Trie_Edge_0_1, Trie<long, MB>* Trie_bag_1, long scalar,
+                                 const std::string& out) {
+  typedef const TrieBlock<hybrid, MB>* TB;
+  Trie<long, MB>* Trie_BarbellSelAgg_ = new Trie<long, MB>(out, 0, true);
+  long result;
+  {
+    ParTrieBuilder<long, MB> Builders(Trie_BarbellSelAgg_, 3);
+    ParTrieIterator<void*, MB> Iterators_Edge_b_c(Trie_Edge_0_1);
+    ParTrieIterator<long, MB> Iterators_bag_1_a(Trie_bag_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_c(Trie_Edge_0_1);
+    ParTrieIterator<void*, MB> Iterators_Edge_a_b(Trie_Edge_0_1);
+    std::vector<TB> a_sets;
+    a_sets.push_back(Iterators_bag_1_a.head);
+    a_sets.push_back(Iterators_Edge_a_c.head);
+    a_sets.push_back(Iterators_Edge_a_b.head);
+    const size_t count_a = Builders.build_aggregated_set(&a_sets);
+    (void)count_a;
+    par::reducer<long> annotation_a(0, [&](long a, long b) { return a + b; });
+    Builders.par_foreach_aggregate([&](const size_t tid, const uint32_t a_d) {
+      TrieBuilder<long, MB>* Builder = Builders.builders.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_b_c = Iterators_Edge_b_c.iterators.at(tid);
+      TrieIterator<long, MB>* Iterator_bag_1_a = Iterators_bag_1_a.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_c = Iterators_Edge_a_c.iterators.at(tid);
+      TrieIterator<void*, MB>* Iterator_Edge_a_b = Iterators_Edge_a_b.iterators.at(tid);
+      Iterator_Edge_a_c->get_next_block(0, a_d);
+      Iterator_Edge_a_b->get_next_block(0, a_d);
+      const size_t count_b =
+          Builder->build_aggregated_set(Iterator_Edge_b_c->get_block(0), Iterator_Edge_a_b->get_block(1));
+      (void)count_b;
+      long annotation_b = (long)0;
+      Builder->foreach_aggregate([&](const uint32_t b_d) {
+        Iterator_Edge_b_c->get_next_block(0, b_d);
+        const size_t count_c =
+            Builder->build_aggregated_set(Iterator_Edge_b_c->get_block(1), Iterator_Edge_a_c->get_block(1));
+        const long intermediate_c = (long)1 * (count_c * 1);
+        annotation_b += intermediate_c;
+      });
+      const long intermediate_a = (long)1 * Iterator_bag_1_a->get_annotation(0, a_d) * annotation_b * scalar;
+      annotation_a.update(tid, intermediate_a);
+    });
+    Builders.trie->annotation = annotation_a.evaluate(0);
+    result = Builders.trie->annotation;
+  }
+  delete Trie_BarbellSelAgg_;
+  return result;
+}
+
 static void put(FILE* f, const void* p, size_t n) { fwrite(p, 1, n, f); }
 
 /* Writes, for the head and for each child set: type, cardinality, range,
@@ -411,6 +636,57 @@ static int setops(const char* inp, const char* outp) {
   return 0;
 }
 
+/* ---- dictionary encoding with the reference's Encoding<T>
+ * (Encoding.cpp:21-48): build over a std::set of every column's values,
+ * then encode_column per column.  Input: u32 type (0 uint32, 1 int,
+ * 2 long, 3 float), u32 n_cols, per column u64 n and n values.  Output:
+ * u32 num_distinct, key_to_value[num_distinct], then u32 keys per column. */
+#include "Encoding.hpp"
+template <class T>
+static int encode_typed(FILE* f, FILE* o, uint32_t n_cols) {
+  std::vector<std::vector<T>> cols(n_cols);
+  std::set<T> values;
+  for (uint32_t c = 0; c < n_cols; c++) {
+    uint64_t n = 0;
+    if (fread(&n, 8, 1, f) != 1) return 1;
+    cols[c].resize(n);
+    if (n && fread(cols[c].data(), sizeof(T), n, f) != n) return 1;
+    values.insert(cols[c].begin(), cols[c].end());
+  }
+  Encoding<T> enc;
+  enc.build(&values);
+  put(o, &enc.num_distinct, 4);
+  for (uint32_t k = 0; k < enc.num_distinct; k++) put(o, &enc.key_to_value.at(k), sizeof(T));
+  for (uint32_t c = 0; c < n_cols; c++) {
+    std::vector<uint32_t>* keys = enc.encode_column(cols[c].data(), cols[c].size());
+    if (!keys->empty()) put(o, keys->data(), 4 * keys->size());
+    delete keys;
+  }
+  return 0;
+}
+
+static int encode_mode(const char* inp, const char* outp) {
+  FILE* f = fopen(inp, "rb");
+  if (!f) return 1;
+  uint32_t hdr[2];
+  if (fread(hdr, 4, 2, f) != 2) { fclose(f); return 1; }
+  FILE* o = fopen(outp, "wb");
+  if (!o) { fclose(f); return 1; }
+  thread_pool::initializeThreadPool();
+  int rc = 2;
+  switch (hdr[0]) {
+    case 0: rc = encode_typed<uint32_t>(f, o, hdr[1]); break;
+    case 1: rc = encode_typed<int>(f, o, hdr[1]); break;
+    case 2: rc = encode_typed<long>(f, o, hdr[1]); break;
+    case 3: rc = encode_typed<float>(f, o, hdr[1]); break;
+  }
+  fclose(f);
+  fclose(o);
+  printf("{\"mode\": \"encode\", \"rc\": %d}\n", rc);
+  fflush(stdout);
+  _exit(rc);
+}
+
 static std::string scratch_dir() {
   const char* t = getenv("TMPDIR");
   std::string base = t ? t : "/tmp";
@@ -424,23 +700,38 @@ static std::string scratch_dir() {
 int main(int argc, char** argv) {
   if (argc < 3) {
     fprintf(stderr, "usage: eh_ref triangle|clique4|lollipop|barbell <edges> [repeats]\n"
+                    "       eh_ref clique4_sel|barbell_sel <edges> <repeats> <value>\n"
                     "       eh_ref trie_dump <edges> <out>\n       eh_ref setops <pairs> <out>\n");
     return 2;
   }
   const std::string mode = argv[1];
   if (mode == "setops") return argc > 3 ? setops(argv[2], argv[3]) : 2;
+  if (mode == "encode") return argc > 3 ? encode_mode(argv[2], argv[3]) : 2;
 
   std::vector<uint32_t> s, d;
   if (!read_edges(argv[2], s, d) || s.empty()) {
     fprintf(stderr, "cannot read edges from %s\n", argv[2]);
     return 1;
   }
-  const uint32_t nd = encode(s, d);
+  std::vector<uint32_t> key_to_value;
+  const uint32_t nd = encode(s, d, key_to_value);
   const std::string dir = scratch_dir();
   thread_pool::initializeThreadPool();
   const double tb0 = now_s();
   Trie<void*, MB>* Trie_Edge_0_1 = build_edge_trie(dir + "/Edge_0_1", s, d, nd);
+  /* selection plans read Edge(a,x) in order [x,a]: the relation's second
+   * trie, columns swapped (createDB.scala builds one per attribute order) */
+  const bool sel_mode = mode == "clique4_sel" || mode == "barbell_sel";
+  Trie<void*, MB>* Trie_Edge_1_0 = sel_mode ? build_edge_trie(dir + "/Edge_1_0", d, s, nd) : nullptr;
   const double build_s = now_s() - tb0;
+  uint32_t sel_key = 0;
+  if (sel_mode) {
+    const uint32_t sel_value = argc > 4 ? (uint32_t)strtoul(argv[4], nullptr, 10) : 0u;
+    if (!value_to_key(key_to_value, sel_value, &sel_key)) {
+      fprintf(stderr, "selection value %u is not in the relation\n", sel_value);
+      return 1;
+    }
+  }
 
   if (mode == "trie_dump") {
     int rc = argc > 3 ? trie_dump(Trie_Edge_0_1, argv[3]) : 2;
@@ -463,6 +754,21 @@ int main(int argc, char** argv) {
       count = mode == "lollipop" ? bag_lollipop_root(Trie_Edge_0_1, bag1, dir + "/LollipopAgg")
                                  : bag_barbell_root(Trie_Edge_0_1, bag1, dir + "/BarbellAgg");
       delete bag1;
+    } else if (mode == "clique4_sel") {
+      Trie<long, MB>* bag1 = bag_selected_partners(Trie_Edge_1_0, sel_key, dir + "/bag_1_x_a_FliqueSelAgg");
+      count = bag1 ? bag_clique4_sel_root(Trie_Edge_0_1, bag1, dir + "/FliqueSelAgg") : 0;
+      delete bag1;
+    } else if (mode == "barbell_sel") {
+      Trie<long, MB>* bag1 = bag_selected_partners(Trie_Edge_1_0, sel_key, dir + "/bag_1_p_a_BarbellSelAgg");
+      Trie<long, MB>* bag2 = bag_selected_partners(Trie_Edge_0_1, sel_key, dir + "/bag_2_p_x_BarbellSelAgg");
+      if (bag1 && bag2) {
+        const long scalar = bag_triangle_sel_scalar(Trie_Edge_0_1, bag2, dir + "/bag_1_x_y_z_BarbellSelAgg");
+        count = bag_barbell_sel_root(Trie_Edge_0_1, bag1, scalar, dir + "/BarbellSelAgg");
+      } else {
+        count = 0;
+      }
+      delete bag1;
+      delete bag2;
     } else {
       fprintf(stderr, "unknown mode %s\n", mode.c_str());
       return 2;

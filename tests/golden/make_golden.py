@@ -193,7 +193,8 @@ def main():
     specs = [("er_16384_131072_s1", lambda: O.gen_er(1, 16384, 131072), ("triangle", "clique4"), False),
              ("rmat_s12_ef16_s3", lambda: O.gen_rmat(3, 12, 16 << 12), ("triangle", "clique4"), False),
              ("rmat_s16_ef16_s42", lambda: O.gen_rmat(42, 16, 16 << 16), ("triangle", "clique4"), False),
-             ("rmat_s14_ef16_s5_sym", lambda: O.gen_rmat(5, 14, 16 << 14), ("triangle", "lollipop", "barbell"), True),
+             ("rmat_s14_ef16_s5_sym", lambda: O.gen_rmat(5, 14, 16 << 14), ("triangle", "lollipop", "barbell", "clique4"),
+              True),
              ("chunglu_n65536_d32_g2.1_s9_sym", lambda: O.gen_chunglu(9, 65536, 65536 * 16, 2.1),
               ("triangle", "lollipop", "barbell"), True)]
     for name, gen, modes, sym in specs:

@@ -148,3 +148,42 @@ def test_triangle_listing_goldens(oracle, facebook):
     # the projected attribute c is not intersected by the reference plan:
     # more rows than the pairs that close a triangle
     assert len(np.unique(rows[:, :2], axis=0)) == 84185
+
+
+def test_selection_goldens(oracle, facebook, golden):
+    """FliqueSelAgg x=0 -> 3759972 and BarbellSelAgg p=6 -> 26936100 on
+    facebook_duplicated (test/graph/travis.py:385-401, 472-487)."""
+    tr = golden["travis"]["facebook_duplicated"]
+    d = facebook["duplicated"]
+    t = oracle.Trie(d[:, 0], d[:, 1])
+    assert t.clique4_sel(0) == tr["clique4_sel_x0"] == 3759972
+    assert t.barbell_sel(6) == tr["barbell_sel_p6"] == 26936100
+
+
+@pytest.mark.parametrize("name", ["facebook_duplicated", "facebook_pruned"] + SMALL)
+def test_selection_vs_reference_engine(oracle, facebook, golden, name):
+    """Selection counts of the compiled reference engine (its selection
+    bags, several selected values per graph) equal the oracle's."""
+    if name.startswith("facebook"):
+        a = facebook[name.split("_")[1]]
+        s, d = a[:, 0], a[:, 1]
+    else:
+        (u, v), sym = _gen(oracle, name)
+        s, d, _ = oracle.preprocess(u, v, symmetric=sym)
+    t = oracle.Trie(s, d)
+    for key, want in golden["select"][name].items():
+        mode, val = key.rsplit("_", 1)
+        assert getattr(t, mode)(int(val)) == want, key
+
+
+def test_encoding_vs_reference(oracle):
+    """The numpy restatement of Encoding<T> equals the reference's own
+    Encoding<T> (fixture from oracle/_ref/eh_ref encode) for every numeric
+    value type: key_to_value table (bit for bit) and every key."""
+    z = np.load(__import__("os").path.join(__import__("conftest").GOLDEN, "encoding.npz"))
+    for vt in oracle.VALUE_TYPES:
+        cols = [z["%s_col%d" % (vt, j)] for j in range(3)]
+        values, keys = oracle.encoding(cols, vt)
+        assert values.tobytes() == z[vt + "_values"].tobytes(), vt
+        for j, k in enumerate(keys):
+            np.testing.assert_array_equal(k, z["%s_keys%d" % (vt, j)])
