@@ -104,6 +104,8 @@ def lib():
                               ctypes.POINTER(_P)],
             "eh_trie_relayout": [_P, _P, ctypes.POINTER(LayoutConfig)],
             "eh_trie_free": [_P],
+            "eh_trie_load_reference": [_P, ctypes.c_char_p, ctypes.POINTER(LayoutConfig), ctypes.POINTER(_P)],
+            "eh_trie_save_reference": [_P, _P, ctypes.c_char_p, ctypes.c_uint32],
             "eh_trie_info_get": [_P, ctypes.POINTER(TrieInfo)],
             "eh_trie_export": [_P, _P, _P, _P, _P],
             "eh_trie_set_bytes": [_P, ctypes.c_uint32, _P, ctypes.c_uint64, _u64p, ctypes.POINTER(ctypes.c_uint8)],
@@ -321,6 +323,24 @@ class Trie:
                                        ctypes.byref(h)))
         self.h = h
         self.ctx._adopt(self)
+
+    @classmethod
+    def load_reference(cls, path, policy=HEURISTIC, forced=UINTEGER, model=None, ctx=None, max_bitset_bytes=0):
+        """Trie<void*,ParMemoryBuffer>::load (Trie.cpp:37-75) of a two-level
+        trie the reference saved under path (path/ram/trieinfo.bin, ...)."""
+        self = cls.__new__(cls)
+        self.ctx = ctx or default_context()
+        cfg = _layout_cfg(policy, forced, model, max_bitset_bytes)
+        h = ctypes.c_void_p()
+        _check(lib().eh_trie_load_reference(self.ctx.h, os.fsencode(path), ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self.ctx._adopt(self)
+        return self
+
+    def save_reference(self, path, num_threads):
+        """Trie::save (Trie.cpp:15-35) in the reference's format, loadable by
+        an engine built with NUM_THREADS == num_threads."""
+        _check(lib().eh_trie_save_reference(self.ctx.h, self.h, os.fsencode(path), int(num_threads)))
 
     def free(self):
         if getattr(self, "h", None):

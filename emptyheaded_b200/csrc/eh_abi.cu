@@ -307,6 +307,31 @@ eh_status eh_trie_free(eh_trie* trie) {
   });
 }
 
+eh_status eh_trie_load_reference(eh_context* ctx, const char* dir, const eh_layout_config* cfg, eh_trie** out) {
+  return guarded([&] {
+    need(ctx && dir && out, "null argument");
+    *out = nullptr;
+    set_device(ctx);
+    auto* t = new eh_trie();
+    try {
+      trie_load_reference(ctx, dir, cfg, t);
+    } catch (...) {
+      delete t;
+      throw;
+    }
+    *out = t;
+  });
+}
+
+eh_status eh_trie_save_reference(eh_context* ctx, const eh_trie* trie, const char* dir, uint32_t num_threads) {
+  return guarded([&] {
+    need(ctx && trie && dir, "null argument");
+    need(trie->ctx == ctx, "trie belongs to another context");
+    set_device(ctx);
+    trie_save_reference(ctx, trie, dir, num_threads);
+  });
+}
+
 eh_status eh_trie_info_get(const eh_trie* trie, eh_trie_info* out) {
   return guarded([&] {
     need(trie && out, "null argument");

@@ -130,6 +130,9 @@ void trie_build_from_csr(eh_context* ctx, eh_trie* t);  // head/off/vals already
 void trie_build_reverse(eh_context* ctx, eh_trie* t);   // dir + reverse level
 void trie_layout(eh_context* ctx, eh_trie* t, const eh_layout_config* cfg);
 void trie_set_bytes(const eh_trie* t, uint32_t set_index, std::vector<uint8_t>& out, uint8_t* layout);
+// the reference's on-disk format (eh_disk.cu)
+void trie_load_reference(eh_context* ctx, const char* dir, const eh_layout_config* cfg, eh_trie* t);
+void trie_save_reference(eh_context* ctx, const eh_trie* t, const char* dir, uint32_t num_threads);
 
 // set operations (eh_setops.cu)
 void set_intersect_batch(eh_context* ctx, const uint32_t* elems, const uint64_t* set_off, uint32_t n_sets,

@@ -175,6 +175,22 @@ eh_status eh_trie_export(const eh_trie* trie, uint32_t* head, uint64_t* off, uin
 eh_status eh_trie_set_bytes(const eh_trie* trie, uint32_t set_index, uint8_t* out, uint64_t cap, uint64_t* nbytes,
                             uint8_t* layout);
 
+/* Trie<void*,ParMemoryBuffer>::load (storage_engine/src/Trie.cpp:37-75) of a
+ * two-level trie the reference saved with Trie::save: dir holds ram/trieinfo.bin,
+ * ram/data_head.bin and ram/data_<i>.bin (ParMemoryBuffer.cpp:64-100,
+ * MemoryBuffer.cpp:104-172).  The sets are decoded on the host in whatever
+ * layout they were saved, and the device trie is built from them with cfg's
+ * layout policy (NULL: the density rule).  Annotations are not read. */
+eh_status eh_trie_load_reference(eh_context* ctx, const char* dir, const eh_layout_config* cfg, eh_trie** out);
+/* Trie::save (Trie.cpp:15-35) of a device trie in the reference's format, so
+ * that Trie<void*,ParMemoryBuffer>::load in an engine built with
+ * NUM_THREADS == num_threads reads it (its head buffer is found at index
+ * NUM_THREADS).  Sets are written in hybrid::build's layout (range bitset when
+ * dense, else uint, layouts/hybrid.hpp:103-111) whatever the device layout;
+ * child blocks go to the num_threads buffers in contiguous runs of head
+ * entries.  Creates dir and dir/ram. */
+eh_status eh_trie_save_reference(eh_context* ctx, const eh_trie* trie, const char* dir, uint32_t num_threads);
+
 /* --------------------------------------------------------------- set ops
  * Pairwise intersection of sets given as sorted uint32 runs in one packed
  * host array: set k is elems[set_off[k] .. set_off[k+1]).  Each set is

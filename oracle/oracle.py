@@ -343,3 +343,171 @@ def ref_encoding(cols, value_type):
         keys.append(np.frombuffer(buf, np.uint32, len(c), pos).copy())
         pos += 4 * len(c)
     return values, keys
+
+
+# ------------------------------------------- reference on-disk trie format
+# Trie<A,M>::save / load (storage_engine/src/Trie.cpp:15-75),
+# ParMemoryBuffer::save / load (src/utils/ParMemoryBuffer.cpp:64-100),
+# MemoryBuffer::save / load (src/utils/MemoryBuffer.cpp:104-172):
+#   <dir>/ram/trieinfo.bin   bool annotated, A annotation, size_t num_rows,
+#                            size_t num_columns, size_t num_buffers,
+#                            size_t head size, size_t size[num_buffers]
+#   <dir>/ram/data_head.bin, data_<i>.bin   "<size> <offset> " + size bytes
+# A block (TrieBlock<hybrid,M>, trie/TrieBlock.hpp): bool is_sparse, then a
+# Set<hybrid> header (u32 cardinality, u32 range = last value, size_t
+# number_of_bytes, u8 type; 24 bytes), the set's bytes, then (head) one
+# NextLevel {int index; size_t offset} per element (sparse) or per value
+# 0..range (dense), common::is_sparse(cardinality, range) deciding.
+
+def _read_buffer(path):
+    with open(path, "rb") as f:
+        raw = f.read()
+    sp1 = raw.index(b" ")
+    sp2 = raw.index(b" ", sp1 + 1)
+    size = int(raw[:sp1])
+    return np.frombuffer(raw, np.uint8, size, sp2 + 1)
+
+
+def _is_sparse(length, rng):
+    return (rng / length) > 128.0 if length > 2 else True
+
+
+def _set_values(buf, off):
+    card, rng = np.frombuffer(buf, np.uint32, 2, off + 1)
+    nb = int(np.frombuffer(buf, np.uint64, 1, off + 9)[0])
+    ty = int(buf[off + 17])
+    data = buf[off + 25: off + 25 + nb]
+    if card == 0:
+        vals = np.zeros(0, np.uint32)
+    elif ty == 1:  # UINTEGER
+        vals = data[: 4 * int(card)].copy().view(np.uint32)
+    elif ty == 0:  # RANGE_BITSET [u64 start][u64 words x W][u32 rank x W]
+        w = (nb - 8) // 12
+        start = int(data[:8].copy().view(np.uint64)[0])
+        words = data[8: 8 + 8 * w].copy().view(np.uint64)
+        bits = np.unpackbits(words.view(np.uint8), bitorder="little").reshape(w, 64)
+        wi, bi = np.nonzero(bits)
+        vals = ((start + wi) * 64 + bi).astype(np.uint32)
+    elif ty == 3:  # BLOCK_BITSET [u32 id][u32 rank][4 x u64] per block
+        nblk = nb // 40
+        rec = data[: 40 * nblk].copy()
+        ids = rec.reshape(nblk, 40)[:, :4].copy().view(np.uint32).ravel()
+        words = rec.reshape(nblk, 40)[:, 8:].copy().view(np.uint64).reshape(nblk, 4)
+        bits = np.unpackbits(words.view(np.uint8), bitorder="little").reshape(nblk, 256)
+        bi, vi = np.nonzero(bits)
+        vals = (ids[bi].astype(np.uint64) * 256 + vi).astype(np.uint32)
+    else:
+        raise ValueError("unknown set type %d" % ty)
+    assert len(vals) == card
+    return vals, int(card), int(rng), nb, ty
+
+
+def read_reference_trie(dirpath):
+    """A two-level trie the reference saved: (head, off, vals, types) with
+    types[i] the stored layout of child set i and types[-1] the head's."""
+    ram = os.path.join(dirpath, "ram")
+    info = open(os.path.join(ram, "trieinfo.bin"), "rb").read()
+    for sa in (8, 4):
+        nbuf = int(np.frombuffer(info, np.uint64, 1, 1 + sa + 16)[0])
+        if len(info) == 1 + sa + 32 + 8 * nbuf:
+            break
+    else:
+        raise ValueError("unrecognised trieinfo.bin")
+    ncols = int(np.frombuffer(info, np.uint64, 1, 1 + sa + 8)[0])
+    assert ncols == 2, "two-level tries only"
+    bufs = [_read_buffer(os.path.join(ram, "data_%d.bin" % i)) for i in range(nbuf)]
+    bufs.append(_read_buffer(os.path.join(ram, "data_head.bin")))
+    head, card, rng, nb, hty = _set_values(bufs[nbuf], 0)
+    nxt = 25 + nb
+    dense = not _is_sparse(card, rng)
+    off = [0]
+    vals, types = [], []
+    for i, v in enumerate(head):
+        e = int(v) if dense else i
+        idx = int(np.frombuffer(bufs[nbuf], np.int32, 1, nxt + 16 * e)[0])
+        boff = int(np.frombuffer(bufs[nbuf], np.uint64, 1, nxt + 16 * e + 8)[0])
+        if idx < 0:
+            child, ty = np.zeros(0, np.uint32), 1
+        else:
+            child, _, _, _, ty = _set_values(bufs[idx], boff)
+        vals.append(child)
+        types.append(ty)
+        off.append(off[-1] + len(child))
+    types.append(hty)
+    return (head.astype(np.uint32), np.array(off, np.uint64),
+            np.concatenate(vals).astype(np.uint32) if vals else np.zeros(0, np.uint32), np.array(types, np.uint8))
+
+
+def _set_bytes_hybrid(a):
+    """hybrid::build (layouts/hybrid.hpp:103-111): bytes and type"""
+    if len(a) == 0:
+        return b"", 1
+    if hybrid_type(a) == 0:
+        return range_bitset(a).tobytes(), 0
+    return np.ascontiguousarray(a, np.uint32).tobytes(), 1
+
+
+def _block(a, with_next=None):
+    a = np.ascontiguousarray(a, np.uint32)
+    data, ty = _set_bytes_hybrid(a)
+    last = int(a[-1]) if len(a) else 0
+    hdr = bytes([1 if _is_sparse(len(a), last) else 0])
+    hdr += np.array([len(a), last], np.uint32).tobytes() + np.uint64(len(data)).tobytes() + bytes([ty]) + bytes(7)
+    return hdr + data
+
+
+def write_reference_trie(dirpath, head, off, vals, rows, num_threads):
+    """The layout this project writes (and its device saver writes byte for
+    byte): child blocks in num_threads buffers, head entries split into
+    contiguous chunks per buffer; the head block and its NextLevel array in
+    the head buffer; trieinfo of a Trie<void*,ParMemoryBuffer>."""
+    ram = os.path.join(dirpath, "ram")
+    os.makedirs(ram, exist_ok=True)
+    nh = len(head)
+    per = (nh + num_threads - 1) // num_threads if nh else 0
+    bufs = [bytearray() for _ in range(num_threads)]
+    loc = []
+    for i in range(nh):
+        b = min(i // per, num_threads - 1) if per else 0
+        loc.append((b, len(bufs[b])))
+        bufs[b] += _block(vals[off[i]: off[i + 1]])
+    hb = bytearray(_block(head))
+    last = int(head[-1]) if nh else 0
+    dense = not _is_sparse(nh, last)
+    n_next = (last + 1) if dense else nh
+    nxt = np.zeros(n_next, dtype=[("index", "<i4"), ("pad", "<u4"), ("offset", "<u8")])
+    nxt["index"] = -1
+    for i in range(nh):
+        e = int(head[i]) if dense else i
+        nxt["index"][e] = loc[i][0]
+        nxt["offset"][e] = loc[i][1]
+    hb += nxt.tobytes()
+
+    def put(name, b):
+        with open(os.path.join(ram, name), "wb") as f:
+            f.write(b"%d %d " % (len(b), len(b)))
+            f.write(bytes(b))
+    put("data_head.bin", hb)
+    for i, b in enumerate(bufs):
+        put("data_%d.bin" % i, b)
+    info = bytes([0]) + np.uint64(0).tobytes() + np.array([rows, 2, num_threads, len(hb)], np.uint64).tobytes()
+    info += np.array([len(b) for b in bufs], np.uint64).tobytes()
+    with open(os.path.join(ram, "trieinfo.bin"), "wb") as f:
+        f.write(info)
+
+
+def ref_save(src, dst, dirpath, threads):
+    """The reference engine's own Trie::save of the Edge trie into dirpath."""
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "edges.bin")
+        write_edge_file(p, src, dst)
+        subprocess.run([REF_BIN, "save", p, dirpath], check=True, capture_output=True,
+                       env=dict(os.environ, EH_REF_THREADS=str(threads), TMPDIR=td))
+
+
+def ref_load_triangle(dirpath, threads):
+    """Trie::load of a saved trie by the reference engine, then TriangleAgg."""
+    with tempfile.TemporaryDirectory() as td:
+        out = subprocess.run([REF_BIN, "load_triangle", dirpath], check=True, capture_output=True, text=True,
+                             env=dict(os.environ, EH_REF_THREADS=str(threads), TMPDIR=td)).stdout
+    return json.loads(out.strip().splitlines()[-1])

@@ -25,6 +25,8 @@
  *   eh_ref trie_dump <edges> <out.bin>      dump the reference trie
  *   eh_ref setops <pairs.bin> <out.bin>     per-pair ops::set_intersect
  *   eh_ref encode <cols.bin> <out.bin>      Encoding<T> build + encode_column
+ *   eh_ref save <edges> <dir>               Trie::save of the Edge trie (dir/ram/)
+ *   eh_ref load_triangle <dir>              Trie::load, then the TriangleAgg bag
  * <edges> is a .tsv (two uint32 columns) or an edge file written by the
  * project's graph generator ("EHEDGE01" header, u64 n, u32 src[n], u32 dst[n]).
  *
@@ -707,6 +709,18 @@ int main(int argc, char** argv) {
   const std::string mode = argv[1];
   if (mode == "setops") return argc > 3 ? setops(argv[2], argv[3]) : 2;
   if (mode == "encode") return argc > 3 ? encode_mode(argv[2], argv[3]) : 2;
+  if (mode == "load_triangle") {
+    /* Trie::load (Trie.cpp:37-75) of a saved Edge trie, then the TriangleAgg bag */
+    thread_pool::initializeThreadPool();
+    Trie<void*, MB>* loaded = Trie<void*, MB>::load(argv[2]);
+    const std::string dir = scratch_dir();
+    const long count = bag_triangle(loaded, dir + "/TriangleAgg");
+    printf("{\"mode\": \"load_triangle\", \"count\": %ld, \"count_u64\": %llu, \"rows\": %zu, "
+           "\"threads\": %zu}\n",
+           count, (unsigned long long)(uint64_t)count, loaded->num_rows, NUM_THREADS);
+    fflush(stdout);
+    _exit(0);
+  }
 
   std::vector<uint32_t> s, d;
   if (!read_edges(argv[2], s, d) || s.empty()) {
@@ -731,6 +745,17 @@ int main(int argc, char** argv) {
       fprintf(stderr, "selection value %u is not in the relation\n", sel_value);
       return 1;
     }
+  }
+
+  if (mode == "save") {
+    /* Trie::save (Trie.cpp:15-35) of the Edge trie into <dir>/ram/ */
+    if (argc < 4) return 2;
+    const std::string out = argv[3];
+    Trie<void*, MB>* saved = build_edge_trie(out, s, d, nd);
+    saved->save();
+    printf("{\"mode\": \"save\", \"rows\": %zu, \"threads\": %zu}\n", s.size(), NUM_THREADS);
+    fflush(stdout);
+    _exit(0);
   }
 
   if (mode == "trie_dump") {

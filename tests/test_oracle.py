@@ -187,3 +187,43 @@ def test_encoding_vs_reference(oracle):
         assert values.tobytes() == z[vt + "_values"].tobytes(), vt
         for j, k in enumerate(keys):
             np.testing.assert_array_equal(k, z["%s_keys%d" % (vt, j)])
+
+
+def _refdb_dirs(tmp, names=None):
+    z = np.load(__import__("os").path.join(__import__("conftest").GOLDEN, "refdb.npz"))
+    os = __import__("os")
+    out = {}
+    for key in z.files:
+        name, fn = key.split("/")
+        if fn == "threads" or (names and name not in names):
+            continue
+        ram = os.path.join(str(tmp), name, "ram")
+        os.makedirs(ram, exist_ok=True)
+        with open(os.path.join(ram, fn), "wb") as f:
+            f.write(z[key].tobytes())
+        out[name] = (os.path.join(str(tmp), name), int(z[name + "/threads"][0]))
+    return out
+
+
+def test_reference_trie_files(oracle, facebook, tmp_path):
+    """The restatement of the on-disk format reads the tries the reference
+    saved (fixture) into the same CSR the oracle builds from the edges, and
+    what it writes the reference engine loads (triangle count unchanged)."""
+    dirs = _refdb_dirs(tmp_path)
+    p = facebook["pruned"]
+    want = {"facebook_pruned": (p[:, 0], p[:, 1])}
+    for name in ("rmat_s12_ef16_s3", "rmat_s14_ef16_s5_sym"):
+        (u, v), sym = _gen(oracle, name)
+        s, d, _ = oracle.preprocess(u, v, symmetric=sym)
+        want[name] = (s, d)
+    for name, (path, thr) in dirs.items():
+        t = oracle.Trie(*want[name])
+        head, off, vals, types = oracle.read_reference_trie(path)
+        np.testing.assert_array_equal(head, t.head)
+        np.testing.assert_array_equal(off, t.off)
+        np.testing.assert_array_equal(vals, t.vals)
+        np.testing.assert_array_equal(types[:-1], t.layouts())
+        if oracle.ref_available():
+            out = str(tmp_path / ("w_" + name))
+            oracle.write_reference_trie(out, t.head, t.off, t.vals, len(t.vals), thr + 1)
+            assert oracle.ref_load_triangle(out, thr + 1)["count_u64"] == t.triangle(), name
