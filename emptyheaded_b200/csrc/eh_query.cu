@@ -38,6 +38,14 @@ constexpr uint32_t kDefaultLongRow = 32;  // rows with at least this many candid
 #define EH_LONG_UNROLL 4
 #endif
 constexpr int kLongUnroll = EH_LONG_UNROLL;  // independent candidate loads per lane per trip
+#ifndef EH_SHORT_UNROLL
+#define EH_SHORT_UNROLL 4
+#endif
+constexpr int kShortUnroll = EH_SHORT_UNROLL;  // flattened (row, element) pairs per lane per trip
+#ifndef EH_WORD_UNROLL
+#define EH_WORD_UNROLL 1
+#endif
+constexpr int kWordUnroll = EH_WORD_UNROLL;  // flattened (row, word) pairs per lane per trip
 // Defaults measured on B200 at R-MAT-22 (4 KB of staging per warp leaves
 // room for 32 resident warps; 32K-probe items amortise staging); the
 // autotuner (emptyheaded_b200/autotune.py) re-picks them per trie.
@@ -294,32 +302,49 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
           abase = aa.off - aa.start;  // word w of N(a) is bs_words[abase + w]
         }
       }
-      uint32_t rows = __ballot_sync(kFull, word_row && whi >= wlo);
+      // the word rows of this batch, flattened into (row, word) pairs over
+      // the lanes like the short element rows below: one trip covers the
+      // words of many rows
+      const uint32_t nw = (word_row && whi >= wlo) ? whi - wlo + 1 : 0u;
       if (word_row) len = 0;  // handled here, not in the element loop
-      while (rows) {
-        const int j = __ffs(rows) - 1;
-        rows &= rows - 1;
-        const uint32_t a_lo = __shfl_sync(kFull, wlo, j), a_hi = __shfl_sync(kFull, whi, j);
-        const uint32_t b0 = __shfl_sync(kFull, v0, j), b1 = __shfl_sync(kFull, v1, j);
-        const uint64_t base = __shfl_sync(kFull, abase, j);
-        const uint32_t src_j = __shfl_sync(kFull, src, j);
-        uint32_t c = 0;
-        for (uint32_t w = a_lo + lane; w <= a_hi; w += 32) {
-          uint64_t m = ~0ull;
-          if (w == (b0 >> 6)) m &= ~0ull << (b0 & 63);
-          if (w == (b1 >> 6)) m &= ~0ull >> (63 - (b1 & 63));
-          const uint64_t bw = (P == P_SBITS) ? st.words[w - st.start] : __ldg(st.words + (w - st.start));
-          uint64_t x = __ldg(t.bs_words + base + w) & bw & m;
-          c += __popcll(x);
+      const uint32_t wincl = warp_incl_scan(nw);
+      const uint32_t wtotal = __shfl_sync(kFull, wincl, 31);
+      const uint32_t wexcl = wincl - nw;
+      for (uint32_t p = 0; p < wtotal; p += 32 * kWordUnroll) {
+        uint64_t x[kWordUnroll];
+        uint32_t wv[kWordUnroll], sj[kWordUnroll];
+#pragma unroll
+        for (int u = 0; u < kWordUnroll; u++) {
+          const uint32_t q = p + 32 * u + lane;
+          const uint32_t j = owner_lane(wincl, q);
+          const uint32_t lo_w = __shfl_sync(kFull, wlo, j), ex = __shfl_sync(kFull, wexcl, j);
+          const uint32_t b0 = __shfl_sync(kFull, v0, j), b1 = __shfl_sync(kFull, v1, j);
+          const uint64_t base = __shfl_sync(kFull, abase, j);
+          sj[u] = (kMode != MODE_COUNT) ? __shfl_sync(kFull, src, j) : 0u;
+          x[u] = 0;
+          wv[u] = 0;
+          if (q < wtotal) {
+            const uint32_t w = lo_w + (q - ex);
+            uint64_t m = ~0ull;
+            if (w == (b0 >> 6)) m &= ~0ull << (b0 & 63);
+            if (w == (b1 >> 6)) m &= ~0ull >> (63 - (b1 & 63));
+            const uint64_t bw = (P == P_SBITS) ? st.words[w - st.start] : __ldg(st.words + (w - st.start));
+            x[u] = __ldg(t.bs_words + base + w) & bw & m;
+            wv[u] = w;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kWordUnroll; u++) {
+          cnt += __popcll(x[u]);
           if (kMode != MODE_COUNT) {
-            while (x) {
-              const uint32_t bit = __ffsll((long long)x) - 1;
-              on_hit<kMode>(t, r, sk, src_j, (w << 6) | bit);
-              x &= x - 1;
+            uint64_t y = x[u];
+            while (y) {
+              const uint32_t bit = __ffsll((long long)y) - 1;
+              on_hit<kMode>(t, r, sk, sj[u], (wv[u] << 6) | bit);
+              y &= y - 1;
             }
           }
         }
-        cnt += c;
       }
     }
     // ---- long element rows: one row at a time across the warp, two
@@ -355,24 +380,22 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
     const uint32_t incl = warp_incl_scan(len);
     const uint32_t total = __shfl_sync(kFull, incl, 31);
     const uint32_t excl = incl - len;
-    for (uint32_t p = 0; p < total; p += 64) {
-      const uint32_t q0 = p + lane, q1 = p + 32 + lane;
-      const uint32_t j0 = owner_lane(incl, q0), j1 = owner_lane(incl, q1);
-      const uint32_t lo0 = __shfl_sync(kFull, lo, j0), ex0 = __shfl_sync(kFull, excl, j0);
-      const uint32_t lo1 = __shfl_sync(kFull, lo, j1), ex1 = __shfl_sync(kFull, excl, j1);
-      uint32_t s0 = 0, s1 = 0;
-      if (kMode != MODE_COUNT) {
-        s0 = __shfl_sync(kFull, src, j0);
-        s1 = __shfl_sync(kFull, src, j1);
+    for (uint32_t p = 0; p < total; p += 32 * kShortUnroll) {
+      uint32_t w[kShortUnroll], sj[kShortUnroll];
+#pragma unroll
+      for (int u = 0; u < kShortUnroll; u++) {
+        const uint32_t q = p + 32 * u + lane;
+        const uint32_t j = owner_lane(incl, q);
+        const uint32_t loj = __shfl_sync(kFull, lo, j), exj = __shfl_sync(kFull, excl, j);
+        sj[u] = (kMode != MODE_COUNT) ? __shfl_sync(kFull, src, j) : 0u;
+        w[u] = q < total ? __ldg(t.vals + loj + (q - exj)) : 0u;
       }
-      const uint32_t w0 = q0 < total ? __ldg(t.vals + lo0 + (q0 - ex0)) : 0;
-      const uint32_t w1 = q1 < total ? __ldg(t.vals + lo1 + (q1 - ex1)) : 0;
-      const uint32_t h0 = q0 < total ? probe<P>(st, w0) : 0u;
-      const uint32_t h1 = q1 < total ? probe<P>(st, w1) : 0u;
-      cnt += h0 + h1;
-      if (kMode != MODE_COUNT) {
-        if (h0) on_hit<kMode>(t, r, sk, s0, w0);
-        if (h1) on_hit<kMode>(t, r, sk, s1, w1);
+#pragma unroll
+      for (int u = 0; u < kShortUnroll; u++) {
+        const uint32_t q = p + 32 * u + lane;
+        const uint32_t h = q < total ? probe<P>(st, w[u]) : 0u;
+        cnt += h;
+        if (kMode != MODE_COUNT && h) on_hit<kMode>(t, r, sk, sj[u], w[u]);
       }
     }
   }
