@@ -207,6 +207,11 @@ __device__ __forceinline__ uint32_t probe(const Staged& s, uint32_t w) {
 // -- the materialized Triangle(a,b,c) of TrieBuilder::build_set.
 enum { MODE_COUNT = 0, MODE_ANNOT = 1, MODE_MAT = 2 };
 
+constexpr int kHot = 4;  // MODE_ANNOT: head entries with block-local counters
+struct Int4 {
+  int32_t v[kHot];
+};
+
 struct Sink {
   unsigned long long* annot;  // MODE_ANNOT
   uint32_t* ma;               // MODE_MAT: output columns
@@ -215,6 +220,8 @@ struct Sink {
   uint64_t base;              // MODE_MAT: first row of this item's slice
   unsigned int* slot;         // MODE_MAT: the warp's running row count (shared)
   uint32_t b;                 // MODE_MAT: value of the staged head entry b
+  const int32_t* hot;         // MODE_ANNOT: the kHot largest sets' head entries (-1: none)
+  unsigned long long* hot_acc;  // MODE_ANNOT: their block-local counts (shared)
 };
 
 // owner lane of flattened pair q: the number of lanes whose inclusive
@@ -229,14 +236,25 @@ __device__ __forceinline__ uint32_t owner_lane(uint32_t incl, uint32_t q) {
   return j;
 }
 
-template <int kMode>
+// kSrcAgg: the caller adds the row source's share of the annotation for a
+// run of hits at once (add_src), so a hit adds only the matched element's
+// share; a hub source in many rows would otherwise take one atomic per hit.
+template <int kMode, bool kSrcAgg = false>
 __device__ __forceinline__ void on_hit(const TrieView& t, const RevView& r, const Sink& sk, uint32_t src,
                                        uint32_t w) {
   if (kMode == MODE_ANNOT) {
     if (r.dir == DIR_SYM) {
-      atomicAdd(sk.annot + src, 2ull);
-      atomicAdd(sk.annot + __ldg(t.head_index + w), 2ull);
-    } else {
+      if (!kSrcAgg) atomicAdd(sk.annot + src, 2ull);
+      // the matched element: a hub is the third vertex of a large share of
+      // all triangles, so the largest sets count in shared memory first
+      const int32_t hx = __ldg(t.head_index + w);
+      int k = 0;
+#pragma unroll
+      for (; k < kHot; k++)
+        if (hx == sk.hot[k]) break;
+      if (k < kHot) atomicAdd(sk.hot_acc + k, 2ull);
+      else atomicAdd(sk.annot + hx, 2ull);
+    } else if (!kSrcAgg) {
       atomicAdd(sk.annot + src, 1ull);
     }
   } else if (kMode == MODE_MAT) {
@@ -258,6 +276,11 @@ __device__ __forceinline__ void on_hit(const TrieView& t, const RevView& r, cons
       sk.mc[o] = w;
     }
   }
+}
+
+template <int kMode>
+__device__ __forceinline__ void add_src(const RevView& r, const Sink& sk, uint32_t src, uint64_t hits) {
+  if (kMode == MODE_ANNOT && hits) atomicAdd(sk.annot + src, (r.dir == DIR_SYM ? 2ull : 1ull) * hits);
 }
 
 // Rows whose source set N(a) is also a range bitset, against a bitset N(b),
@@ -335,12 +358,14 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
         }
 #pragma unroll
         for (int u = 0; u < kWordUnroll; u++) {
-          cnt += __popcll(x[u]);
-          if (kMode != MODE_COUNT) {
+          const uint32_t hits = __popcll(x[u]);
+          cnt += hits;
+          if (kMode == MODE_ANNOT) add_src<kMode>(r, sk, sj[u], hits);
+          if (kMode == MODE_MAT || (kMode == MODE_ANNOT && r.dir == DIR_SYM)) {
             uint64_t y = x[u];
             while (y) {
               const uint32_t bit = __ffsll((long long)y) - 1;
-              on_hit<kMode>(t, r, sk, sj[u], (wv[u] << 6) | bit);
+              on_hit<kMode, true>(t, r, sk, sj[u], (wv[u] << 6) | bit);
               y &= y - 1;
             }
           }
@@ -361,6 +386,7 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
         uint32_t src_j = 0;
         if (kMode != MODE_COUNT) src_j = __shfl_sync(kFull, src, j);
         const uint32_t* row = t.vals + rlo;
+        uint32_t row_hits = 0;
         for (uint32_t i = lane; i < rn; i += 32 * kLongUnroll) {
           uint32_t w[kLongUnroll];
 #pragma unroll
@@ -369,10 +395,15 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
           for (int u = 0; u < kLongUnroll; u++) {
             if (i + 32 * u < rn) {
               const uint32_t h = probe<P>(st, w[u]);
-              cnt += h;
-              if (kMode != MODE_COUNT && h) on_hit<kMode>(t, r, sk, src_j, w[u]);
+              row_hits += h;
+              if (kMode != MODE_COUNT && h) on_hit<kMode, true>(t, r, sk, src_j, w[u]);
             }
           }
+        }
+        cnt += row_hits;
+        if (kMode == MODE_ANNOT) {  // the row's source once per row
+          const uint32_t rh = warp_sum(row_hits);
+          if (lane == 0) add_src<kMode>(r, sk, src_j, rh);
         }
       }
     }
@@ -395,7 +426,13 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
         const uint32_t q = p + 32 * u + lane;
         const uint32_t h = q < total ? probe<P>(st, w[u]) : 0u;
         cnt += h;
-        if (kMode != MODE_COUNT && h) on_hit<kMode>(t, r, sk, sj[u], w[u]);
+        if (kMode == MODE_ANNOT) {
+          // lanes of one row are adjacent: one source atomic per row present
+          const uint32_t grp = __match_any_sync(kFull, sj[u]);
+          const uint32_t hm = __ballot_sync(kFull, h) & grp;
+          if (lane == (uint32_t)(__ffs(grp) - 1)) add_src<kMode>(r, sk, sj[u], __popc(hm));
+        }
+        if (kMode != MODE_COUNT && h) on_hit<kMode, true>(t, r, sk, sj[u], w[u]);
       }
     }
   }
@@ -453,6 +490,7 @@ struct QueryOut {
   const unsigned long long* item_off;  // MODE_MAT: first output row of each item
   uint32_t *ma, *mb, *mc;      // MODE_MAT: output columns
   const uint32_t* sel;         // 4-clique: bit per node value of a selected partner set, or null
+  int32_t hot[kHot];           // MODE_ANNOT on a symmetric relation: largest sets' head entries, -1 if none
   uint32_t* gsbuf;             // 4-clique: per-warp S buffers in global memory (sets too large for
   uint32_t gcap;               //   shared memory), gcap words each; null: S in shared memory
 };
@@ -464,6 +502,15 @@ __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict_
                                                         int cap_words, QueryOut out) {
   extern __shared__ uint32_t smem[];
   __shared__ unsigned int slot[kMaxWarps];  // MODE_MAT: rows written by the warp's item so far
+  __shared__ unsigned long long hot_acc[kHot];
+  __shared__ int32_t hot[kHot];
+  if (kMode == MODE_ANNOT) {
+    if (threadIdx.x < kHot) {
+      hot_acc[threadIdx.x] = 0;
+      hot[threadIdx.x] = out.hot[threadIdx.x];
+    }
+    __syncthreads();
+  }
   const uint32_t lane = lane_id();
   const uint32_t wid = threadIdx.x >> 5;
   uint32_t* sm = smem + (size_t)wid * cap_words;
@@ -486,7 +533,7 @@ __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict_
     const RevView r = revs[item.g];
     long long t0 = 0;
     if (out.records && lane == 0) t0 = clock64();
-    Sink sk{out.annot, out.ma, out.mb, out.mc, 0, &slot[wid], 0};
+    Sink sk{out.annot, out.ma, out.mb, out.mc, 0, &slot[wid], 0, hot, hot_acc};
     if (kMode == MODE_MAT) {
       if (lane == 0) slot[wid] = 0;
       __syncwarp();
@@ -525,6 +572,11 @@ __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict_
     }
   }
   if (lane == 0 && cur_g != 0xffffffffu && acc) atomicAdd(out.total + cur_g, acc);
+  if (kMode == MODE_ANNOT) {  // every warp leaves the loop above; then flush the block's hot counts
+    __syncthreads();
+    if (threadIdx.x < kHot && hot[threadIdx.x] >= 0 && hot_acc[threadIdx.x])
+      atomicAdd(out.annot + hot[threadIdx.x], hot_acc[threadIdx.x]);
+  }
 }
 
 // ------------------------------------------------------------ 4-clique
@@ -662,11 +714,14 @@ __global__ void EH_TRI_LAUNCH_BOUNDS clique4_kernel(const TrieView* __restrict__
 }
 
 // ------------------------------------------------- lollipop / barbell roots
+constexpr uint64_t kRootBig = 32768;  // barbell root: larger sets get grid-wide passes
+
 // LollipopAgg root, order [a,d]: sum_a T(a) * |N(a)|
-// BarbellAgg root, order [a,x]: sum_a T(a) * sum_{x in N(a) ∩ head} T(x)
+// BarbellAgg root, order [a,x]: sum_a T(a) * sum_{x in N(a) ∩ head} T(x);
+// Tv = T by value (0 off the head): one random load per row instead of two
 template <bool kBarbell>
 __global__ void root_kernel(TrieView t, const unsigned long long* __restrict__ T,
-                            unsigned long long* __restrict__ total) {
+                            const unsigned long long* __restrict__ Tv, unsigned long long* __restrict__ total) {
   const uint32_t lane = lane_id();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -674,12 +729,10 @@ __global__ void root_kernel(TrieView t, const unsigned long long* __restrict__ T
   for (uint32_t a = warp; a < t.n_head; a += nwarps) {
     const unsigned long long ta = T[a];
     if (!ta) continue;
+    if (kBarbell && t.off[a + 1] - t.off[a] > kRootBig) continue;  // root_big_kernel's
     unsigned long long s = 0;
     if (kBarbell) {
-      for (uint64_t e = t.off[a] + lane; e < t.off[a + 1]; e += 32) {
-        const int32_t hx = __ldg(t.head_index + __ldg(t.vals + e));
-        if (hx >= 0) s += T[hx];
-      }
+      for (uint64_t e = t.off[a] + lane; e < t.off[a + 1]; e += 32) s += __ldg(Tv + __ldg(t.vals + e));
       s = warp_sum(s);
     } else {
       s = t.off[a + 1] - t.off[a];
@@ -687,6 +740,31 @@ __global__ void root_kernel(TrieView t, const unsigned long long* __restrict__ T
     acc += ta * s;
   }
   if (lane == 0 && acc) atomicAdd(total, acc);
+}
+
+// the barbell root of one large set a, grid-wide
+__global__ void root_big_kernel(TrieView t, uint32_t a, const unsigned long long* __restrict__ T,
+                                const unsigned long long* __restrict__ Tv, unsigned long long* __restrict__ total) {
+  const unsigned long long ta = T[a];
+  unsigned long long s = 0;
+  for (uint64_t e = t.off[a] + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < t.off[a + 1];
+       e += (uint64_t)gridDim.x * blockDim.x)
+    s += __ldg(Tv + __ldg(t.vals + e));
+  s = warp_sum(s);
+  if (lane_id() == 0 && s) atomicAdd(total, ta * s);
+}
+
+__global__ void root_big_sets_kernel(TrieView t, uint32_t* __restrict__ idx, unsigned int* __restrict__ n) {
+  for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < t.n_head; a += gridDim.x * blockDim.x)
+    if (t.off[a + 1] - t.off[a] > kRootBig) idx[atomicAdd(n, 1u)] = a;
+}
+
+__global__ void t_by_value_kernel(TrieView t, const unsigned long long* __restrict__ T,
+                                  unsigned long long* __restrict__ Tv) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < t.n_nodes; v += gridDim.x * blockDim.x) {
+    const int32_t h = t.head_index[v];
+    Tv[v] = h >= 0 ? T[h] : 0ull;
+  }
 }
 
 // ---------------------------------------------------------------- driver
@@ -729,7 +807,40 @@ struct Prepared {
   uint32_t plan_launches = 0;
   const uint32_t* sel = nullptr;  // 4-clique selection bitmap (QueryOut::sel)
   DevBuf<uint32_t> gs;            // 4-clique global S buffers (ExecParams::s_cap)
+  int32_t hot[kHot] = {-1, -1, -1, -1};  // annotation: largest sets (QueryOut::hot)
 };
+
+// head entry with the largest set, excluding `ex` (-1 unused): max over
+// (size << 32 | position)
+__global__ void top_set_kernel(const uint64_t* __restrict__ off, uint32_t nh, Int4 ex,
+                               unsigned long long* __restrict__ best) {
+  unsigned long long m = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nh; i += gridDim.x * blockDim.x) {
+    if ((int32_t)i == ex.v[0] || (int32_t)i == ex.v[1] || (int32_t)i == ex.v[2] || (int32_t)i == ex.v[3]) continue;
+    m = max(m, (unsigned long long)(((off[i + 1] - off[i]) << 32) | i));
+  }
+  for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(kFull, m, o));
+  if (lane_id() == 0 && m) atomicMax(best, m);
+}
+
+// the kHot head entries with the largest sets of a trie (-1 where fewer)
+static void hot_sets(eh_context* ctx, const eh_trie* t, int32_t* hot) {
+  cudaStream_t s = ctx->stream;
+  Int4 ex{{-1, -1, -1, -1}};
+  DevBuf<unsigned long long> best(1, s);
+  for (int k = 0; k < kHot; k++) hot[k] = -1;
+  for (int k = 0; k < kHot && (uint32_t)k < t->n_head; k++) {
+    EH_CUDA(cudaMemsetAsync(best.p, 0, 8, s));
+    top_set_kernel<<<num_sms() * 4, 256, 0, s>>>(t->off.p, t->n_head, ex, best.p);
+    EH_CHECK_LAUNCH();
+    unsigned long long h = 0;
+    EH_CUDA(cudaMemcpyAsync(&h, best.p, 8, cudaMemcpyDeviceToHost, s));
+    EH_CUDA(cudaStreamSynchronize(s));
+    if (!h) break;
+    hot[k] = (int32_t)(h & 0xffffffffu);
+    ex.v[k] = hot[k];
+  }
+}
 
 static void prepare(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query, ExecParams ep, bool annot,
                     Prepared& P) {
@@ -797,6 +908,7 @@ static void prepare(eh_context* ctx, const eh_trie* const* tries, uint32_t n, in
   }
   const int per_sm = blocks_per_sm(kfn, P.threads, P.smem);
   P.grid = std::max(1, std::min(num_sms() * per_sm, (int)((total_items + ep.warps - 1) / ep.warps)));
+  if (annot && n == 1 && tries[0]->dir == DIR_SYM) hot_sets(ctx, tries[0], P.hot);
   if (query == EH_QUERY_CLIQUE4 && ep.s_cap) {
     // one S buffer per resident warp, at most 2 GiB in all
     const uint64_t per_block = (uint64_t)ep.warps * ep.s_cap * 4;
@@ -817,6 +929,7 @@ static void launch(eh_context* ctx, Prepared& P, unsigned long long* d_total, un
   const ExecParams& ep = P.ep;
   QueryOut out{ep.shard_index, ep.shard_count, ep.long_row, d_total, d_annot, d_records, P.q.p, P.q.p + 1};
   out.sel = P.sel;
+  for (int k = 0; k < kHot; k++) out.hot[k] = P.hot[k];
   out.gsbuf = ep.s_cap ? P.gs.p : nullptr;
   out.gcap = ep.s_cap;
   if (P.query == EH_QUERY_CLIQUE4)
@@ -928,10 +1041,33 @@ void query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t 
     EH_CUDA(cudaMemsetAsync(dummy.p, 0, 8, s));
     L = run_plans(ctx, tries, 1, EH_QUERY_TRIANGLE, ep, true, dummy.p, T.p, nullptr, &items, &pairs);
     if (t->n_head) {
-      if (query == EH_QUERY_LOLLIPOP)
-        root_kernel<false><<<num_sms() * 8, 256, 0, s>>>(t->view(), T.p, total.p);
-      else
-        root_kernel<true><<<num_sms() * 8, 256, 0, s>>>(t->view(), T.p, total.p);
+      if (query == EH_QUERY_LOLLIPOP) {
+        root_kernel<false><<<num_sms() * 8, 256, 0, s>>>(t->view(), T.p, nullptr, total.p);
+      } else {
+        DevBuf<unsigned long long> Tv(t->n_nodes ? t->n_nodes : 1, s);
+        t_by_value_kernel<<<num_sms() * 8, 256, 0, s>>>(t->view(), T.p, Tv.p);
+        root_kernel<true><<<num_sms() * 8, 256, 0, s>>>(t->view(), T.p, Tv.p, total.p);
+        EH_CHECK_LAUNCH();
+        L.launches++;
+        if (t->info.max_set > kRootBig) {
+          DevBuf<uint32_t> idx(t->n_head, s);
+          DevBuf<unsigned int> nb(1, s);
+          EH_CUDA(cudaMemsetAsync(nb.p, 0, 4, s));
+          root_big_sets_kernel<<<num_sms() * 4, 256, 0, s>>>(t->view(), idx.p, nb.p);
+          EH_CHECK_LAUNCH();
+          unsigned int hn = 0;
+          EH_CUDA(cudaMemcpyAsync(&hn, nb.p, 4, cudaMemcpyDeviceToHost, s));
+          EH_CUDA(cudaStreamSynchronize(s));
+          std::vector<uint32_t> big(hn);
+          if (hn) EH_CUDA(cudaMemcpyAsync(big.data(), idx.p, 4ull * hn, cudaMemcpyDeviceToHost, s));
+          EH_CUDA(cudaStreamSynchronize(s));
+          for (uint32_t a : big) {
+            root_big_kernel<<<num_sms() * 4, 256, 0, s>>>(t->view(), a, T.p, Tv.p, total.p);
+            EH_CHECK_LAUNCH();
+          }
+          L.launches += 1 + hn;
+        }
+      }
       EH_CHECK_LAUNCH();
       L.launches++;
     }

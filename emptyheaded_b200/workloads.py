@@ -27,3 +27,18 @@ def build_rmat_trie(E, scale, seed, ctx=None, symmetric=False, **trie_kw):
     s.free()
     d.free()
     return t
+
+
+def build_chunglu_trie(E, n=1 << 23, avg_degree=32, gamma=2.1, seed=9, ctx=None, **trie_kw):
+    """Device pipeline for the barbell / lollipop workload: Chung-Lu power
+    law with n nodes and n * avg_degree / 2 undirected samples, symmetrised
+    and deduplicated (the reference runs these plans on the duplicated
+    relation, test/graph/travis.py:647-692)."""
+    u, v = E.gen_chunglu(seed, n, n * avg_degree // 2, gamma, ctx=ctx)
+    s, d, nodes = E.preprocess(u, v, symmetric=True, ctx=ctx)
+    u.free()
+    v.free()
+    t = E.Trie(s, d, ctx=ctx, **trie_kw)
+    s.free()
+    d.free()
+    return t
