@@ -160,7 +160,11 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint64_t
   counts[(uint64_t)threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// kVals: a uint32 payload travels with each key (read at write time)
+// kVals: a uint32 payload travels with each key.  The tile's keys are first
+// placed in digit order in shared memory (stable: tile digit start + the
+// warp's offset within the digit + the key's rank in its warp), then written
+// out in that order, so consecutive threads write consecutive slots of one
+// digit's run (coalesced) instead of 256 scattered runs per round.
 template <bool kVals>
 __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint64_t* __restrict__ keys,
                                                                      uint64_t* __restrict__ out, uint64_t n,
@@ -171,12 +175,17 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint6
                                                                      uint32_t* __restrict__ vout) {
   __shared__ uint32_t whist[kSortWarps][kRadix];
   __shared__ uint32_t tile_off[kRadix];
+  __shared__ uint32_t tstart[kRadix];
+  __shared__ uint32_t wtot[kSortWarps];
+  extern __shared__ uint64_t skeys[];  // kSortTile keys, then (kVals) kSortTile uint32 payloads
+  uint32_t* svals = reinterpret_cast<uint32_t*>(skeys + kSortTile);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&whist[0][0])[i] = 0;
   tile_off[threadIdx.x] = offsets[(uint64_t)threadIdx.x * tiles + blockIdx.x];
   __syncthreads();
   // warp w owns keys [base + w*512, base + (w+1)*512), round-major
-  const uint64_t wbase = (uint64_t)blockIdx.x * kSortTile + (uint64_t)wid * (32 * kSortRounds);
+  const uint64_t tbase = (uint64_t)blockIdx.x * kSortTile;
+  const uint64_t wbase = tbase + (uint64_t)wid * (32 * kSortRounds);
   uint64_t k[kSortRounds];
   uint32_t pos[kSortRounds];
   const uint32_t lt = lanemask_lt();
@@ -197,28 +206,44 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint6
     pos[r] = basecnt + rank;  // offset among this warp's keys of digit d
   }
   __syncthreads();
-  // per-digit exclusive prefix over warps (thread t owns digit t)
-  {
-    uint32_t run = 0;
+  // per-digit exclusive prefix over warps (thread t owns digit t), and the
+  // tile's digit starts (exclusive scan over digits)
+  uint32_t run = 0;
 #pragma unroll
-    for (int w = 0; w < kSortWarps; w++) {
-      uint32_t c = whist[w][threadIdx.x];
-      whist[w][threadIdx.x] = run;
-      run += c;
-    }
+  for (int w = 0; w < kSortWarps; w++) {
+    const uint32_t c = whist[w][threadIdx.x];
+    whist[w][threadIdx.x] = run;
+    run += c;
   }
+  const uint32_t inc = warp_incl_scan(run);
+  if (lane == 31) wtot[wid] = inc;
+  __syncthreads();
+  uint32_t before = 0;
+  for (int w = 0; w < wid; w++) before += wtot[w];
+  tstart[threadIdx.x] = before + inc - run;
   __syncthreads();
 #pragma unroll
   for (int r = 0; r < kSortRounds; r++) {
     const uint64_t i = wbase + (uint64_t)r * 32 + lane;
     if (i < n) {
       const uint32_t d = (uint32_t)((k[r] >> shift) & 0xff);
-      const uint32_t dst = tile_off[d] + whist[wid][d] + pos[r];
-      out[dst] = k[r];
-      if (kVals) vout[dst] = vin[i];
+      const uint32_t li = tstart[d] + whist[wid][d] + pos[r];
+      skeys[li] = k[r];
+      if (kVals) svals[li] = vin[i];
     }
   }
+  __syncthreads();
+  const uint32_t cnt = (uint32_t)min((uint64_t)kSortTile, n - tbase);
+  for (uint32_t j = threadIdx.x; j < cnt; j += kSortThreads) {
+    const uint64_t key = skeys[j];
+    const uint32_t d = (uint32_t)((key >> shift) & 0xff);
+    const uint32_t dst = tile_off[d] + (j - tstart[d]);
+    out[dst] = key;
+    if (kVals) vout[dst] = svals[j];
+  }
 }
+
+static size_t scatter_smem(bool vals) { return (size_t)kSortTile * (8 + (vals ? 4 : 0)); }
 
 // LSD passes; with vals != nullptr a uint32 payload follows its key (stable)
 static void radix_sort_impl(uint64_t* keys, uint64_t* tmp, uint32_t* vals, uint32_t* vtmp, uint64_t n, int bits,
@@ -227,6 +252,14 @@ static void radix_sort_impl(uint64_t* keys, uint64_t* tmp, uint32_t* vals, uint3
   EH_REQUIRE(n < (1ull << 32), EH_ERR_UNSUPPORTED, "radix sort supports fewer than 2^32 keys");
   const uint32_t tiles = (uint32_t)((n + kSortTile - 1) / kSortTile);
   DevBuf<uint32_t> counts((uint64_t)kRadix * tiles, s);
+  static bool smem_set = false;  // the staged scatter takes more than the default 48 KB
+  if (!smem_set) {
+    EH_CUDA(cudaFuncSetAttribute(radix_scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)scatter_smem(true)));
+    EH_CUDA(cudaFuncSetAttribute(radix_scatter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)scatter_smem(false)));
+    smem_set = true;
+  }
   uint64_t* src = keys;
   uint64_t* dst = tmp;
   uint32_t* vsrc = vals;
@@ -236,10 +269,11 @@ static void radix_sort_impl(uint64_t* keys, uint64_t* tmp, uint32_t* vals, uint3
     EH_CHECK_LAUNCH();
     exclusive_scan<uint32_t>(counts.p, counts.p, (uint64_t)kRadix * tiles, nullptr, s);
     if (vals)
-      radix_scatter_kernel<true><<<tiles, kSortThreads, 0, s>>>(src, dst, n, shift, counts.p, tiles, vsrc, vdst);
+      radix_scatter_kernel<true><<<tiles, kSortThreads, scatter_smem(true), s>>>(src, dst, n, shift, counts.p, tiles,
+                                                                                vsrc, vdst);
     else
-      radix_scatter_kernel<false><<<tiles, kSortThreads, 0, s>>>(src, dst, n, shift, counts.p, tiles, nullptr,
-                                                                  nullptr);
+      radix_scatter_kernel<false><<<tiles, kSortThreads, scatter_smem(false), s>>>(src, dst, n, shift, counts.p,
+                                                                                  tiles, nullptr, nullptr);
     EH_CHECK_LAUNCH();
     std::swap(src, dst);
     std::swap(vsrc, vdst);
