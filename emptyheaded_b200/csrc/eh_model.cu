@@ -8,7 +8,7 @@
 // the time of a set under each layout, and EH_POLICY_LEARNED gives every
 // set the layout with the lowest predicted time.  The density rule stays
 // as the fallback (sets the model cannot place, memory cap) and as the
-// judge in the tests.  Layouts change speed only: every layout holds the
+// point of comparison in the tests.  Layouts change speed only: every layout holds the
 // same elements, so counts are identical.
 //
 // Network: widths d0 -> d1 -> ... -> dL, ReLU between layers, linear

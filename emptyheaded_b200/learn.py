@@ -10,7 +10,7 @@ its own kernels) to predict log cycles from the set's features and a
 layout; EH_POLICY_LEARNED then gives each set its predicted-cheapest
 layout.  The reference's density rule (common::is_sparse,
 utils/common.hpp:60-66) stays as the fallback for sets the plan never
-stages and as the judge: `evaluate` reports the model's prediction error
+stages and as the point of comparison: `evaluate` reports the model's prediction error
 and the regret of both policies against the exhaustive search.
 """
 import numpy as np
