@@ -79,6 +79,12 @@ struct eh_trie {
   eh::DevBuf<uint32_t> rev_src;   // head position of a for entry k
   eh::DevBuf<uint64_t> rev_wpre;  // exclusive prefix of entry work, rev_entries + 1 values
   uint64_t rev_entries = 0, rev_pairs = 0;
+  // With learned layouts: the cost model's predicted SM cycles of every
+  // staged set's work (0 for sets never staged), and their sum over the
+  // probes; the planner cuts work items by predicted cycles instead of
+  // probes, so items are uniform in time.
+  eh::DevBuf<float> work_pred;
+  double pred_per_probe = 0;
   eh_trie_info info{};
 
   eh::TrieView view() const {
@@ -170,6 +176,6 @@ void encoding_free(eh_encoding* e);
 
 // learned layout policy (eh_model.cu)
 void model_choose_layouts(eh_context* ctx, const eh_model* m, const eh_trie* t, uint64_t max_bitset_bytes,
-                          uint8_t* layout_dev);
+                          uint8_t* layout_dev, float* pred_dev);
 
 }  // namespace eh

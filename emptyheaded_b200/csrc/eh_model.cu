@@ -173,11 +173,13 @@ __device__ __forceinline__ void model_features(const TrieView& t, uint32_t b, ui
 // 48x the set's uint bytes in the worst case.
 __global__ void choose_kernel(TrieView t, const uint64_t* __restrict__ rev_off, const uint64_t* __restrict__ wpre,
                               const float* __restrict__ params, const int* __restrict__ dims, int L,
-                              const int* __restrict__ woff, uint64_t max_words_per_set, uint8_t* __restrict__ layout) {
+                              const int* __restrict__ woff, uint64_t max_words_per_set, uint8_t* __restrict__ layout,
+                              float* __restrict__ pred) {
   float buf0[64], buf1[64];
   for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.n_head; b += gridDim.x * blockDim.x) {
     const uint64_t s0 = t.off[b];
     const uint32_t len = (uint32_t)(t.off[b + 1] - s0);
+    if (pred) pred[b] = 0.f;
     if (!len) continue;
     const uint64_t pairs = wpre[rev_off[b + 1]] - wpre[rev_off[b]];
     if (!pairs) continue;  // never staged: keep the fallback layout
@@ -212,11 +214,12 @@ __global__ void choose_kernel(TrieView t, const uint64_t* __restrict__ rev_off, 
       }
     }
     layout[b] = (uint8_t)best_l;
+    if (pred) pred[b] = fmaxf(expm1f(best), 1.f);  // the model predicts log1p(cycles)
   }
 }
 
 void model_choose_layouts(eh_context* ctx, const eh_model* m, const eh_trie* t, uint64_t max_bitset_bytes,
-                          uint8_t* layout_dev) {
+                          uint8_t* layout_dev, float* pred_dev) {
   cudaStream_t s = ctx->stream;
   EH_REQUIRE(m->dims[0] == kFeat && m->dims[m->n_layers] == 1, EH_ERR_INVALID,
              "layout model must map 6 features to 1 output");
@@ -228,7 +231,7 @@ void model_choose_layouts(eh_context* ctx, const eh_model* m, const eh_trie* t, 
   EH_CUDA(cudaMemcpyAsync(ddims.p, m->dims.data(), (m->n_layers + 1) * 4, cudaMemcpyHostToDevice, s));
   EH_CUDA(cudaMemcpyAsync(dwoff.p, woff.data(), m->n_layers * 4, cudaMemcpyHostToDevice, s));
   choose_kernel<<<num_sms() * 2, 128, 0, s>>>(t->view(), t->rev_off.p, t->rev_wpre.p, m->params.p, ddims.p,
-                                               m->n_layers, dwoff.p, max_bitset_bytes / 12, layout_dev);
+                                               m->n_layers, dwoff.p, max_bitset_bytes / 12, layout_dev, pred_dev);
   EH_CHECK_LAUNCH();
   EH_CUDA(cudaStreamSynchronize(s));
 }

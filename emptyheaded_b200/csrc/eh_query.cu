@@ -97,6 +97,20 @@ __global__ void plan_count_kernel(RevView r, uint32_t nh, uint32_t chunk, uint32
     nitems[b] = (uint32_t)((w + chunk - 1) / chunk);
   }
 }
+// the same from the cost model's predicted cycles of b's work (learned
+// layouts): items of about `unit` predicted cycles, at most one per 64 probes
+__global__ void plan_count_pred_kernel(RevView r, uint32_t nh, const float* __restrict__ pred, double unit,
+                                       uint32_t* __restrict__ nitems) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nh; b += gridDim.x * blockDim.x) {
+    const uint64_t w = r.rev_wpre[r.rev_off[b + 1]] - r.rev_wpre[r.rev_off[b]];
+    uint64_t n = 0;
+    if (w) {
+      n = (uint64_t)ceil((double)pred[b] / unit);
+      n = max((uint64_t)1, min(n, (w + 63) / 64));
+    }
+    nitems[b] = (uint32_t)n;
+  }
+}
 // item i of b covers the rows whose work prefix falls in [i, i+1) * W/n;
 // items are written in reverse head order so the queue starts at the
 // largest-degree b (ids are degree-ordered) and small items come last
@@ -139,7 +153,10 @@ static void build_plan(eh_context* ctx, const eh_trie* t, uint32_t chunk, uint32
   RevView r{t->rev_off.p, t->rev_lo.p, t->rev_hi.p, t->rev_src.p, t->rev_wpre.p, t->dir};
   DevBuf<uint32_t> nitems(t->n_head, s), ipos(t->n_head, s), tot(1, s);
   const int grid = num_sms() * 4;
-  plan_count_kernel<<<grid, 256, 0, s>>>(r, t->n_head, chunk, nitems.p);
+  if (t->work_pred.p && t->pred_per_probe > 0)
+    plan_count_pred_kernel<<<grid, 256, 0, s>>>(r, t->n_head, t->work_pred.p, t->pred_per_probe * chunk, nitems.p);
+  else
+    plan_count_kernel<<<grid, 256, 0, s>>>(r, t->n_head, chunk, nitems.p);
   EH_CHECK_LAUNCH();
   exclusive_scan<uint32_t>(nitems.p, ipos.p, t->n_head, tot.p, s);
   uint32_t n = 0;

@@ -308,6 +308,13 @@ __global__ void layout_hist_kernel(const uint8_t* __restrict__ layout, uint32_t 
     atomicAdd(&hist[layout[i] & 3], 1u);
 }
 
+__global__ void sum_f32_kernel(const float* __restrict__ a, uint32_t n, double* __restrict__ sum) {
+  double v = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v += a[i];
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  if (lane_id() == 0 && v != 0) atomicAdd(sum, v);
+}
+
 static SetSrc set_src(const eh_trie* t) { return SetSrc{t->head.p, t->off.p, t->vals.p, t->n_head}; }
 
 // Build the probe structures for the layouts in t->layout.
@@ -430,7 +437,7 @@ static void update_bytes(eh_trie* t) {
                          t->layout.bytes() + t->aux.bytes() + t->bs_words.bytes() + t->bs_rank.bytes() +
                          t->bb_id.bytes() + t->bb_rank.bytes() + t->bb_words.bytes() + t->wedges.bytes() +
                          t->rev_off.bytes() + t->rev_lo.bytes() + t->rev_hi.bytes() + t->rev_src.bytes() +
-                         t->rev_wpre.bytes();
+                         t->rev_wpre.bytes() + t->work_pred.bytes();
 }
 
 void trie_layout(eh_context* ctx, eh_trie* t, const eh_layout_config* cfg) {
@@ -448,9 +455,22 @@ void trie_layout(eh_context* ctx, eh_trie* t, const eh_layout_config* cfg) {
   layout_heuristic_kernel<<<num_sms() * 4, 256, 0, s>>>(set_src(t), n_sets, policy, forced, max_words,
                                                          t->layout.p);
   EH_CHECK_LAUNCH();
+  t->work_pred.release();
+  t->pred_per_probe = 0;
   if (policy == EH_POLICY_LEARNED) {
     EH_REQUIRE(cfg->model != nullptr, EH_ERR_INVALID, "learned layout policy needs a model");
-    model_choose_layouts(ctx, cfg->model, t, cfg->max_bitset_bytes, t->layout.p);
+    if (t->n_head && t->rev_pairs) t->work_pred.alloc(t->n_head, s);
+    model_choose_layouts(ctx, cfg->model, t, cfg->max_bitset_bytes, t->layout.p, t->work_pred.p);
+    if (t->work_pred.p) {
+      DevBuf<double> sum(1, s);
+      EH_CUDA(cudaMemsetAsync(sum.p, 0, 8, s));
+      sum_f32_kernel<<<num_sms() * 4, 256, 0, s>>>(t->work_pred.p, t->n_head, sum.p);
+      EH_CHECK_LAUNCH();
+      double h = 0;
+      EH_CUDA(cudaMemcpyAsync(&h, sum.p, 8, cudaMemcpyDeviceToHost, s));
+      EH_CUDA(cudaStreamSynchronize(s));
+      t->pred_per_probe = h / (double)t->rev_pairs;
+    }
   }
   ph.end();
   TracePhase ph_s("layout.structs", s);
