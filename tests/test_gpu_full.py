@@ -55,3 +55,29 @@ def test_rmat22_triangle_count_every_layout(eh, rmat22):
     ann = t.triangle_annotation()
     assert int(ann.sum(dtype=np.uint64)) == g["triangle"]
     t.free()
+
+
+def test_chunglu23_lollipop_barbell_match_reference(eh, golden):
+    """Barbell / lollipop configuration at full size: Chung-Lu n = 2^23,
+    average degree 32, exponent 2.1, symmetrised (221,539,750 rows).  The
+    device pipeline gives the edge list the reference engine counted (sha1),
+    and the triangle, lollipop and barbell counts equal the reference's;
+    the annotation sums to the triangle count (a second code path)."""
+    g = golden["synthetic"]["chunglu_n8388608_d32_g2.1_s9_sym"]
+    n = 1 << 23
+    u, v = eh.gen_chunglu(9, n, n * 16, 2.1)
+    s, d, nn = eh.preprocess(u, v, symmetric=True)
+    u.free()
+    v.free()
+    hs, hd = s.numpy(), d.numpy()
+    assert (len(hs), nn) == (g["rows"], g["nodes"])
+    assert hashlib.sha1(hs.tobytes() + hd.tobytes()).hexdigest() == g["sha1"]
+    del hs, hd
+    t = eh.Trie(s, d)
+    s.free()
+    d.free()
+    assert t.count("triangle") == g["triangle"]
+    assert t.count("lollipop") == g["lollipop"]
+    assert t.count("barbell") == g["barbell"]
+    assert int(t.triangle_annotation().sum(dtype=np.uint64)) == g["triangle"]
+    t.free()
