@@ -298,7 +298,8 @@ def ours_arm(args):
             ev.append(1e3 * (time.perf_counter() - a))
             assert c == g["triangle"]
         e2e = {"value": statistics.median(ev), "unit": "ms", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8,
-               "path": "eh_query_count_host_csr: pinned host CSR -> device, trie index + layouts, count, result to host"}
+               "path": "eh_query_count_host_csr: pinned host CSR -> device, trie index + layouts, count, result to host",
+               "runs_ms": [round(x, 2) for x in ev]}
 
     # ---- CPU baseline (rank 0, N = 1): the reference engine on the same rows
     cpu = None

@@ -35,6 +35,7 @@ HEURISTIC, LEARNED, FORCED = 0, 1, 2
 QUERIES = {"triangle": 0, "clique4": 1, "lollipop": 2, "barbell": 3}
 # equality-selection plans (Trie.count_select)
 SELECT_QUERIES = {"clique4_sel": 4, "barbell_sel": 5}
+QUERY_NAMES = {v: k for k, v in list(QUERIES.items()) + list(SELECT_QUERIES.items())}
 
 
 class EHError(RuntimeError):
@@ -60,6 +61,15 @@ class ExecConfig(ctypes.Structure):
     _fields_ = [("warps_per_block", ctypes.c_int), ("chunk_pairs", ctypes.c_int), ("long_row", ctypes.c_int),
                 ("smem_words", ctypes.c_int), ("record_timings", ctypes.c_int), ("spin_limit", ctypes.c_uint64),
                 ("shard_index", ctypes.c_int), ("shard_count", ctypes.c_int)]
+
+
+class Atom(ctypes.Structure):
+    _fields_ = [("relation", ctypes.c_uint32), ("v0", ctypes.c_uint32), ("v1", ctypes.c_uint32)]
+
+
+class Rule(ctypes.Structure):
+    _fields_ = [("n_vars", ctypes.c_uint32), ("n_atoms", ctypes.c_uint32), ("atoms", ctypes.c_void_p),
+                ("sel_var", ctypes.c_int32), ("sel_value", ctypes.c_uint32)]
 
 
 class QueryStats(ctypes.Structure):
@@ -118,6 +128,9 @@ def lib():
             "eh_encoding_free": [_P],
             "eh_query_count": [_P, _P, ctypes.c_int, ctypes.POINTER(ExecConfig), _u64p, ctypes.POINTER(QueryStats)],
             "eh_query_count_noalloc": [_P, _P, ctypes.c_int, ctypes.POINTER(ExecConfig), _u64p],
+            "eh_rule_match": [ctypes.POINTER(Rule), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_uint32)],
+            "eh_rule_count": [_P, _P, ctypes.c_uint32, ctypes.POINTER(Rule), ctypes.POINTER(ExecConfig), _u64p,
+                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(QueryStats)],
             "eh_query_count_select": [_P, _P, ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ExecConfig), _u64p,
                                       ctypes.POINTER(QueryStats)],
             "eh_query_materialize": [_P, _P, ctypes.c_int, ctypes.POINTER(ExecConfig), ctypes.c_int, _P, _P, _P,

@@ -443,6 +443,29 @@ eh_status eh_encoding_free(eh_encoding* enc) {
   });
 }
 
+eh_status eh_rule_match(const eh_rule* rule, int* query, uint32_t* relation) {
+  return guarded([&] {
+    need(rule && query, "null argument");
+    *query = rule_match(rule, relation);
+  });
+}
+
+eh_status eh_rule_count(eh_context* ctx, const eh_trie* const* relations, uint32_t n_relations, const eh_rule* rule,
+                        const eh_exec_config* cfg, uint64_t* result, int* query, eh_query_stats* stats) {
+  return guarded([&] {
+    need(ctx && relations && rule && result, "null argument");
+    uint32_t rel = 0;
+    const int q = rule_match(rule, &rel);
+    need(rel < n_relations && relations[rel], "rule names a relation that was not given");
+    set_device(ctx);
+    if (q == EH_QUERY_CLIQUE4_SEL || q == EH_QUERY_BARBELL_SEL)
+      query_count_select(ctx, relations[rel], q, rule->sel_value, cfg, result, stats);
+    else
+      query_count(ctx, relations[rel], q, cfg, result, stats);
+    if (query) *query = q;
+  });
+}
+
 eh_status eh_query_count_select(eh_context* ctx, const eh_trie* trie, int query, uint32_t value,
                                 const eh_exec_config* cfg, uint64_t* result, eh_query_stats* stats) {
   return guarded([&] {

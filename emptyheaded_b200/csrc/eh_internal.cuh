@@ -162,6 +162,9 @@ void query_count_in_scratch(eh_context* ctx, const eh_trie* t, int query, const 
 void query_materialize(eh_context* ctx, const eh_trie* t, int query, const eh_exec_config* cfg, int n_cols,
                        uint32_t* a, uint32_t* b, uint32_t* c, uint64_t cap, uint64_t* n_rows);
 
+// rules (eh_rule.cu): the EH_QUERY_* of a rule body, and its relation
+int rule_match(const eh_rule* rule, uint32_t* relation);
+
 // dictionary encoding (eh_encode.cu)
 eh_encoding* encoding_build(eh_context* ctx, const void* const* cols, const uint64_t* n_rows, uint32_t n_cols,
                             int type, int on_device);

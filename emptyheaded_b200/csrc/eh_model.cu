@@ -218,6 +218,87 @@ __global__ void choose_kernel(TrieView t, const uint64_t* __restrict__ rev_off, 
   }
 }
 
+// choose_kernel for the default network (6 -> 32 -> 32 -> 1): the weights
+// live in shared memory (broadcast reads), the first hidden layer in
+// registers, and the second is folded into the output one unit at a time, so
+// no activation array touches local memory.
+constexpr int kH = 32;
+constexpr int kFixedParams = kH * kFeat + kH + kH * kH + kH + kH + 1;
+
+__device__ __forceinline__ float mlp_fixed(const float* __restrict__ P, float f0, float f1, float f2, float f3,
+                                           float f4, float f5) {
+  const float* W0 = P;
+  const float* b0 = W0 + kH * kFeat;
+  const float* W1 = b0 + kH;
+  const float* b1 = W1 + kH * kH;
+  const float* W2 = b1 + kH;
+  float h1[kH];
+#pragma unroll
+  for (int o = 0; o < kH; o++) {
+    const float* w = W0 + o * kFeat;
+    float z = b0[o];
+    z = fmaf(w[0], f0, z);
+    z = fmaf(w[1], f1, z);
+    z = fmaf(w[2], f2, z);
+    z = fmaf(w[3], f3, z);
+    z = fmaf(w[4], f4, z);
+    z = fmaf(w[5], f5, z);
+    h1[o] = fmaxf(z, 0.f);
+  }
+  float y = W2[kH];
+#pragma unroll 2
+  for (int o = 0; o < kH; o++) {
+    const float* w = W1 + o * kH;
+    float z = b1[o];
+#pragma unroll
+    for (int i = 0; i < kH; i++) z = fmaf(w[i], h1[i], z);
+    y = fmaf(W2[o], fmaxf(z, 0.f), y);
+  }
+  return y;
+}
+
+__global__ void __launch_bounds__(128) choose_fixed_kernel(TrieView t, const uint64_t* __restrict__ rev_off,
+                                                           const uint64_t* __restrict__ wpre,
+                                                           const float* __restrict__ params,
+                                                           uint64_t max_words_per_set, uint8_t* __restrict__ layout,
+                                                           float* __restrict__ pred) {
+  __shared__ float P[kFixedParams];
+  for (int i = threadIdx.x; i < kFixedParams; i += blockDim.x) P[i] = params[i];
+  __syncthreads();
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.n_head; b += gridDim.x * blockDim.x) {
+    if (pred) pred[b] = 0.f;
+    const uint64_t s0 = t.off[b];
+    const uint32_t len = (uint32_t)(t.off[b + 1] - s0);
+    if (!len) continue;
+    const uint64_t pairs = wpre[rev_off[b + 1]] - wpre[rev_off[b]];
+    if (!pairs) continue;  // never staged: keep the fallback layout
+    const uint32_t first = t.vals[s0], last = t.vals[s0 + len - 1];
+    const uint32_t words = (last >> 6) - (first >> 6) + 1;
+    const uint32_t range = last - first;
+    // the features of model_features; the layout one-hot varies per candidate
+    const float f0 = log1pf((float)len), f1 = log1pf((float)range), f2 = (float)len / ((float)range + 1.f),
+                f3 = log1pf((float)pairs);
+    float best = mlp_fixed(P, f0, f1, f2, f3, 0.f, 0.f);  // uint
+    int best_l = EH_LAYOUT_UINTEGER;
+    if (!((uint64_t)words > 16ull * len + 64 || (max_words_per_set && words > max_words_per_set))) {
+      const float y = mlp_fixed(P, f0, f1, f2, f3, 1.f, 0.f);  // range bitset
+      if (y < best) {
+        best = y;
+        best_l = EH_LAYOUT_RANGE_BITSET;
+      }
+    }
+    {
+      const float y = mlp_fixed(P, f0, f1, f2, f3, 0.f, 1.f);  // block bitset
+      if (y < best) {
+        best = y;
+        best_l = EH_LAYOUT_BLOCK_BITSET;
+      }
+    }
+    layout[b] = (uint8_t)best_l;
+    if (pred) pred[b] = fmaxf(expm1f(best), 1.f);  // the model predicts log1p(cycles)
+  }
+}
+
 void model_choose_layouts(eh_context* ctx, const eh_model* m, const eh_trie* t, uint64_t max_bitset_bytes,
                           uint8_t* layout_dev, float* pred_dev) {
   cudaStream_t s = ctx->stream;
@@ -225,6 +306,13 @@ void model_choose_layouts(eh_context* ctx, const eh_model* m, const eh_trie* t, 
              "layout model must map 6 features to 1 output");
   EH_REQUIRE(m->max_dim <= 64, EH_ERR_INVALID, "layout model layers must be at most 64 wide");
   if (!t->n_head || !t->rev_entries) return;
+  if (m->n_layers == 3 && m->dims[1] == kH && m->dims[2] == kH && (int)m->n_params == kFixedParams) {
+    choose_fixed_kernel<<<num_sms() * 4, 128, 0, s>>>(t->view(), t->rev_off.p, t->rev_wpre.p, m->params.p,
+                                                      max_bitset_bytes / 12, layout_dev, pred_dev);
+    EH_CHECK_LAUNCH();
+    EH_CUDA(cudaStreamSynchronize(s));
+    return;
+  }
   std::vector<int> woff(m->n_layers);
   for (int l = 0; l < m->n_layers; l++) woff[l] = (int)m->w_off[l];
   DevBuf<int> ddims(m->n_layers + 1, s), dwoff(m->n_layers, s);

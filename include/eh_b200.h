@@ -270,6 +270,36 @@ eh_status eh_query_count_noalloc(eh_context* ctx, const eh_trie* trie, int query
 eh_status eh_query_count_select(eh_context* ctx, const eh_trie* trie, int query, uint32_t value,
                                 const eh_exec_config* cfg, uint64_t* result, eh_query_stats* stats);
 
+/* A COUNT rule given as data, the bag-level entry the generated code can
+ * call instead of a named plan: the rule body's atoms over numbered
+ * variables (relation index, first and second variable; rel(v0, v1) holds
+ * for the rows (v0, v1) of relation `relation`) and an optional equality
+ * selection (sel_var >= 0: that variable = sel_value).  Replaces the
+ * query compiler's plan + emitted bag (QueryPlanner, EHGenerator.scala:
+ * 728-838) for the bodies the device runs: a COUNT does not depend on the
+ * attribute order or the bag decomposition, nor on the names of the
+ * variables, so the body is matched up to renaming against the triangle,
+ * 4-clique, lollipop and barbell bodies and the 4-clique / barbell
+ * selections of test/graph/travis.py.  Other bodies, or atoms over more than
+ * one relation, are EH_ERR_UNSUPPORTED. */
+typedef struct {
+  uint32_t relation;
+  uint32_t v0, v1;
+} eh_atom;
+typedef struct {
+  uint32_t n_vars;
+  uint32_t n_atoms;
+  const eh_atom* atoms;
+  int32_t sel_var; /* -1: no selection */
+  uint32_t sel_value;
+} eh_rule;
+/* the device plan (EH_QUERY_*) of a rule and the relation it reads; host only */
+eh_status eh_rule_match(const eh_rule* rule, int* query, uint32_t* relation);
+/* COUNT of a rule over relations[] (tries in ordering [0,1]); *query gets
+ * the plan it ran (may be NULL) */
+eh_status eh_rule_count(eh_context* ctx, const eh_trie* const* relations, uint32_t n_relations, const eh_rule* rule,
+                        const eh_exec_config* cfg, uint64_t* result, int* query, eh_query_stats* stats);
+
 /* Materialized output of the triangle plan, rows sorted lexicographically
  * (the order Trie::foreach, storage_engine/src/Trie.cpp:130-160, walks the
  * reference's output trie).  Replaces the materializing bag of
