@@ -257,7 +257,27 @@ def ours_arm(args):
     learn_info = {}
     cfg_l = cfg_h
     try:
-        model, learn_info = train_layout_model(E, trie)
+        if world > 1:
+            # every rank must cut the same plan from the same layouts and
+            # predicted costs: rank 0 trains the model, the others load its
+            # parameters (the same collectives on every rank, failure included)
+            from emptyheaded_b200 import learn as LN
+            ok = torch.zeros(1, device="cuda")
+            model = E.Model(LN.DIMS, ctx=ctx)
+            if rank == 0:
+                try:
+                    model, learn_info = train_layout_model(E, trie)
+                    ok.fill_(1)
+                except Exception as ex:
+                    learn_info = {"error": repr(ex)[:300]}
+            torch.distributed.broadcast(ok, 0)
+            if ok.item() != 1:
+                raise RuntimeError("cost model training failed on rank 0")
+            p = torch.from_numpy(model.params()).cuda()
+            torch.distributed.broadcast(p, 0)
+            model.set_params(p.cpu().numpy())
+        else:
+            model, learn_info = train_layout_model(E, trie)
         trie.relayout(policy=E.LEARNED, model=model)
         info_l = trie.info()
         cfg_l, tlog_l = tune(trie)
