@@ -239,6 +239,15 @@ struct Sink {
   uint32_t b;                 // MODE_MAT: value of the staged head entry b
   const int32_t* hot;         // MODE_ANNOT: the kHot largest sets' head entries (-1: none)
   unsigned long long* hot_acc;  // MODE_ANNOT: their block-local counts (shared)
+  // MODE_ANNOT on a symmetric relation: every matched element is in the
+  // staged N(b); when it is staged with room to spare, each element has a
+  // shared counter (wcnt, by position in N(b)) flushed once per item
+  uint32_t* wcnt;             // null: matched elements go to the annotation directly
+  int wmode;                  // P_SLIST (position by search) or P_SBITS (position by rank)
+  const uint32_t* wlist;      // P_SLIST: the staged list, wn elements
+  const uint64_t* wwords;     // P_SBITS: the staged words, wn of them from word wstart
+  const uint32_t* wrank;      // P_SBITS: elements before each staged word
+  uint32_t wstart, wn;
 };
 
 // owner lane of flattened pair q: the number of lanes whose inclusive
@@ -262,6 +271,22 @@ __device__ __forceinline__ void on_hit(const TrieView& t, const RevView& r, cons
   if (kMode == MODE_ANNOT) {
     if (r.dir == DIR_SYM) {
       if (!kSrcAgg) atomicAdd(sk.annot + src, 2ull);
+      if (sk.wcnt) {  // the matched element's position in the staged N(b)
+        uint32_t pos;
+        if (sk.wmode == P_SLIST) {
+          uint32_t lo = 0, hi = sk.wn;
+          while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sk.wlist[mid] < w) lo = mid + 1; else hi = mid;
+          }
+          pos = lo;
+        } else {
+          const uint32_t idx = (w >> 6) - sk.wstart;
+          pos = sk.wrank[idx] + (uint32_t)__popcll(sk.wwords[idx] & ((1ull << (w & 63)) - 1));
+        }
+        atomicAdd(sk.wcnt + pos, 1u);
+        return;
+      }
       // the matched element: a hub is the third vertex of a large share of
       // all triangles, so the largest sets count in shared memory first
       const int32_t hx = __ldg(t.head_index + w);
@@ -550,7 +575,8 @@ __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict_
     const RevView r = revs[item.g];
     long long t0 = 0;
     if (out.records && lane == 0) t0 = clock64();
-    Sink sk{out.annot, out.ma, out.mb, out.mc, 0, &slot[wid], 0, hot, hot_acc};
+    Sink sk{out.annot, out.ma, out.mb, out.mc, 0, &slot[wid], 0, hot, hot_acc, nullptr, 0, nullptr, nullptr,
+            nullptr, 0, 0};
     if (kMode == MODE_MAT) {
       if (lane == 0) slot[wid] = 0;
       __syncwarp();
@@ -559,6 +585,28 @@ __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict_
     }
     Staged st;
     const int mode = stage_set(t, item.hb, sm, cap_words, st);
+    const uint64_t b0 = t.off[item.hb];
+    const uint32_t blen = (uint32_t)(t.off[item.hb + 1] - b0);
+    if (kMode == MODE_ANNOT && r.dir == DIR_SYM && (mode == P_SLIST || mode == P_SBITS)) {
+      // per-element counters after the staged structure, if they fit
+      const uint32_t used = mode == P_SLIST ? st.n : 3 * st.n;  // list, or words (2 per) + ranks
+      if (used + blen <= (uint32_t)cap_words) {
+        sk.wmode = mode;
+        sk.wn = st.n;
+        sk.wlist = st.list;
+        sk.wwords = st.words;
+        sk.wstart = st.start;
+        if (mode == P_SBITS) {
+          uint32_t* rk = sm + 2 * st.n;
+          const uint32_t* grk = t.bs_rank + t.aux[item.hb].off;
+          for (uint32_t j = lane; j < st.n; j += 32) rk[j] = __ldg(grk + j);
+          sk.wrank = rk;
+        }
+        sk.wcnt = sm + used;
+        for (uint32_t j = lane; j < blen; j += 32) sk.wcnt[j] = 0;
+        __syncwarp();
+      }
+    }
     uint64_t c;
     switch (mode) {
       case P_SBITS: c = stream_rows<P_SBITS, kMode>(st, t, r, item.kb, item.ke, out.long_row, sk); break;
@@ -568,6 +616,13 @@ __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict_
       default: c = stream_rows<P_GBLOCK, kMode>(st, t, r, item.kb, item.ke, out.long_row, sk); break;
     }
     c = warp_sum(c);
+    if (kMode == MODE_ANNOT && sk.wcnt) {  // flush the item's per-element counts
+      __syncwarp();
+      for (uint32_t j = lane; j < blen; j += 32) {
+        const uint32_t n = sk.wcnt[j];
+        if (n) atomicAdd(out.annot + __ldg(t.head_index + __ldg(t.vals + b0 + j)), 2ull * n);
+      }
+    }
     if (kMode == MODE_ANNOT && r.dir == DIR_SYM && lane == 0 && c) atomicAdd(out.annot + item.hb, 2ull * c);
     if (out.item_counts && lane == 0) out.item_counts[it] = c * out.count_mult;
     acc += c;
