@@ -303,9 +303,22 @@ __global__ void set_size_stats_kernel(const uint64_t* __restrict__ off, uint32_t
   }
 }
 
+// sets per layout code: per-thread counts, warp sums, one atomic per warp
+// and code (a global atomic per set on four addresses serialised at L2)
 __global__ void layout_hist_kernel(const uint8_t* __restrict__ layout, uint32_t n, uint32_t* __restrict__ hist) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    atomicAdd(&hist[layout[i] & 3], 1u);
+  uint32_t c[4] = {0, 0, 0, 0};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t l = layout[i] & 3;
+    c[0] += l == 0;
+    c[1] += l == 1;
+    c[2] += l == 2;
+    c[3] += l == 3;
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint32_t v = warp_sum(c[k]);
+    if (lane_id() == 0 && v) atomicAdd(&hist[k], v);
+  }
 }
 
 __global__ void sum_f32_kernel(const float* __restrict__ a, uint32_t n, double* __restrict__ sum) {
@@ -323,6 +336,7 @@ static void build_layout_structs(eh_context* ctx, eh_trie* t) {
   const uint32_t n_sets = t->n_head + 1;
   const int grid = num_sms() * 8;
   SetSrc src = set_src(t);
+  TracePhase ph_size("structs.sizes", s);
   t->aux.alloc(n_sets, s);
   DevBuf<uint64_t> words(n_sets + 1, s), blocks(n_sets + 1, s), tot(2, s);
   aux_size_kernel<<<grid, 256, 0, s>>>(src, n_sets, t->layout.p, t->aux.p, words.p, blocks.p);
@@ -371,6 +385,8 @@ static void build_layout_structs(eh_context* ctx, eh_trie* t) {
   uint64_t h[2];
   EH_CUDA(cudaMemcpyAsync(h, tot.p, 16, cudaMemcpyDeviceToHost, s));
   EH_CUDA(cudaStreamSynchronize(s));
+  ph_size.end();
+  TracePhase ph_fill("structs.bitset_fill", s);
   t->bs_words.alloc(h[0] ? h[0] : 1, s);
   t->bs_rank.alloc(h[0] ? h[0] : 1, s);
   t->bb_id.alloc(h[1] ? h[1] : 1, s);
@@ -380,11 +396,15 @@ static void build_layout_structs(eh_context* ctx, eh_trie* t) {
     bitset_fill_kernel<<<grid, 256, 0, s>>>(src, n_sets, t->layout.p, t->aux.p, t->bs_words.p, t->bs_rank.p);
     EH_CHECK_LAUNCH();
   }
+  ph_fill.end();
+  TracePhase ph_bfill("structs.block_fill", s);
   if (h[1]) {
     block_fill_kernel<<<grid, 256, 0, s>>>(src, n_sets, t->layout.p, t->aux.p, t->bb_id.p, t->bb_rank.p,
                                            t->bb_words.p);
     EH_CHECK_LAUNCH();
   }
+  ph_bfill.end();
+  TracePhase ph_big("structs.big_sets", s);
   for (size_t k = 0; k < big.size(); k++) {
     const uint32_t i = big[k];
     SetAux a{};
@@ -411,6 +431,8 @@ static void build_layout_structs(eh_context* ctx, eh_trie* t) {
       EH_CHECK_LAUNCH();
     }
   }
+  ph_big.end();
+  TracePhase ph_hist("structs.hist", s);
   DevBuf<uint32_t> hist(4, s);
   EH_CUDA(cudaMemsetAsync(hist.p, 0, 16, s));
   if (t->n_head) {
