@@ -99,6 +99,9 @@ def lib():
             "eh_context_destroy": [_P],
             "eh_context_sync": [_P],
             "eh_context_stream": [_P, ctypes.POINTER(_P)],
+            "eh_context_memory": [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                  ctypes.POINTER(ctypes.c_uint64)],
+            "eh_context_reserve": [_P, ctypes.c_uint64],
             "eh_device_alloc": [_P, ctypes.c_uint64, ctypes.POINTER(_P)],
             "eh_device_free": [_P, _P],
             "eh_memcpy": [_P, _P, _P, ctypes.c_uint64],
@@ -211,6 +214,18 @@ class Context:
         s = ctypes.c_void_p()
         _check(lib().eh_context_stream(self.h, ctypes.byref(s)))
         return s.value
+
+    def memory(self):
+        """{reserved, used, peak} bytes of the engine's device memory pool
+        (eh_context_memory); peak counts since the last reserve()."""
+        r, u, p = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().eh_context_memory(self.h, ctypes.byref(r), ctypes.byref(u), ctypes.byref(p)))
+        return {"reserved": r.value, "used": u.value, "peak": p.value}
+
+    def reserve(self, nbytes):
+        """Keep nbytes of device memory in the pool as one block
+        (eh_context_reserve): calls whose peak fits then map no new memory."""
+        _check(lib().eh_context_reserve(self.h, ctypes.c_uint64(int(nbytes))))
 
 
 @atexit.register

@@ -38,20 +38,52 @@ cudaMemPool_t device_pool() {
   return g_pools[dev];
 }
 
-bool trace_enabled() {
-  static const bool on = [] {
+int trace_mode() {
+  static const int mode = [] {
     const char* e = getenv("EH_TRACE");
-    return e && *e && strcmp(e, "0") != 0;
+    if (!e || !*e || strcmp(e, "0") == 0) return 0;
+    return strcmp(e, "2") == 0 ? 2 : 1;
   }();
-  return on;
+  return mode;
 }
+
+bool trace_enabled() { return trace_mode() != 0; }
 
 static double wall_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-TracePhase::TracePhase(const char* n, cudaStream_t st) : name(n), s(st), on(trace_enabled()) {
+static double pool_reserved_gb() {
+  int dev = 0;
+  uint64_t reserved = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxPoolDevices && g_pools[dev])
+    cudaMemPoolGetAttribute(g_pools[dev], cudaMemPoolAttrReservedMemCurrent, &reserved);
+  return reserved / 1e9;
+}
+
+namespace {
+// event-timed phases of the current thread's outermost traced call
+struct EventPhase {
+  const char* name;
+  int depth;
+  cudaEvent_t a, b;
+  double host_ms;
+};
+thread_local std::vector<EventPhase> t_phases;
+thread_local int t_depth = 0;
+}  // namespace
+
+TracePhase::TracePhase(const char* n, cudaStream_t st) : name(n), s(st), mode(trace_mode()), on(mode != 0) {
   if (!on) return;
+  if (mode == 2) {
+    cudaEvent_t a = nullptr;
+    cudaEventCreate(&a);
+    cudaEventRecord(a, s);
+    idx = (int)t_phases.size();
+    t_phases.push_back({n, t_depth++, a, nullptr, 0});
+    t0 = wall_ms();
+    return;
+  }
   cudaStreamSynchronize(s);
   t0 = wall_ms();
 }
@@ -59,8 +91,32 @@ TracePhase::TracePhase(const char* n, cudaStream_t st) : name(n), s(st), on(trac
 void TracePhase::end() {
   if (!on) return;
   on = false;
+  if (mode == 2) {
+    // no synchronisation until the outermost phase ends: the stream runs as
+    // it does untraced, and the events give each phase's device time
+    cudaEvent_t b = nullptr;
+    cudaEventCreate(&b);
+    cudaEventRecord(b, s);
+    t_phases[idx].b = b;
+    t_phases[idx].host_ms = wall_ms() - t0;
+    if (--t_depth == 0) {
+      cudaEventSynchronize(b);
+      for (const EventPhase& p : t_phases) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        fprintf(stderr, "eh-trace %*s%-*s %9.3f ms device %9.3f ms host\n", 2 * p.depth, "", 24 - 2 * p.depth,
+                p.name, ms, p.host_ms);
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+      }
+      fprintf(stderr, "eh-trace pool %.3f GB\n", pool_reserved_gb());
+      t_phases.clear();
+    }
+    return;
+  }
   cudaStreamSynchronize(s);
-  fprintf(stderr, "eh-trace %-24s %9.3f ms\n", name, wall_ms() - t0);
+  // the engine pool's reserved bytes: a phase that grew it paid for new pages
+  fprintf(stderr, "eh-trace %-24s %9.3f ms  pool %.3f GB\n", name, wall_ms() - t0, pool_reserved_gb());
 }
 
 void trim_device_pool(int device) {
@@ -146,6 +202,46 @@ eh_status eh_context_destroy(eh_context* ctx) {
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     trim_device_pool(ctx->device);  // return the pool's unused blocks to the driver
     delete ctx;
+  });
+}
+
+eh_status eh_context_memory(eh_context* ctx, uint64_t* reserved, uint64_t* used, uint64_t* peak) {
+  return guarded([&] {
+    need(ctx, "ctx is null");
+    set_device(ctx);
+    cudaMemPool_t pool = device_pool();
+    uint64_t r = 0, u = 0, h = 0;
+    EH_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r));
+    EH_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u));
+    EH_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &h));
+    if (reserved) *reserved = r;
+    if (used) *used = u;
+    if (peak) *peak = h;
+  });
+}
+
+eh_status eh_context_reserve(eh_context* ctx, uint64_t bytes) {
+  return guarded([&] {
+    need(ctx, "ctx is null");
+    set_device(ctx);
+    cudaMemPool_t pool = device_pool();
+    EH_CUDA(cudaStreamSynchronize(ctx->stream));
+    // unused blocks go back to the driver, then one block of the requested
+    // size is taken and freed: the pool keeps it (release threshold is
+    // unbounded) and carves later allocations out of it
+    EH_CUDA(cudaMemPoolTrimTo(pool, 0));
+    if (bytes) {
+      void* p = nullptr;
+      cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, ctx->stream);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error{EH_ERR_OOM, "reserving " + std::to_string(bytes) + " bytes failed"};
+      }
+      EH_CUDA(cudaFreeAsync(p, ctx->stream));
+      EH_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    uint64_t zero = 0;
+    EH_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero));
   });
 }
 

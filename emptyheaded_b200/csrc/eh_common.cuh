@@ -53,14 +53,19 @@ inline int num_sms() {
 // ---------------------------------------------------------------- tracing
 // Phase timings on stderr when the environment variable EH_TRACE is set,
 // like the reference's timer::start_clock / stop_clock prints
-// (storage_engine/include/utils/timer.hpp:11-20).  A traced phase
+// (storage_engine/include/utils/timer.hpp:11-20).  EH_TRACE=1: a traced phase
 // synchronises its stream when it begins and ends and reports the wall time
-// between; with EH_TRACE unset it costs one branch.
+// between.  EH_TRACE=2: phases record CUDA events instead, nothing
+// synchronises, and the outermost phase prints every phase's device time (and
+// the host time spent inside it) when it ends.  With EH_TRACE unset it costs
+// one branch.
 bool trace_enabled();
 struct TracePhase {
   const char* name;
   cudaStream_t s;
   double t0 = 0;
+  int mode;
+  int idx = -1;
   bool on;
   TracePhase(const char* n, cudaStream_t st);
   ~TracePhase() { end(); }

@@ -74,6 +74,15 @@ eh_status eh_context_destroy(eh_context* ctx);
 eh_status eh_context_sync(eh_context* ctx);
 /* the cudaStream_t the context launches on */
 eh_status eh_context_stream(eh_context* ctx, void** stream);
+/* Engine memory pool of the context's device (no counterpart in the
+ * reference, which allocates from the host heap per call): bytes the pool
+ * holds, bytes in use, and the peak in use since the last reserve. */
+eh_status eh_context_memory(eh_context* ctx, uint64_t* reserved, uint64_t* used, uint64_t* peak);
+/* Returns the pool's unused memory to the driver and reserves `bytes` as one
+ * block that later allocations are carved from, so that calls whose peak fits
+ * never map new device memory (which costs milliseconds per call when the
+ * pool's free blocks are too fragmented for a request).  Resets the peak. */
+eh_status eh_context_reserve(eh_context* ctx, uint64_t bytes);
 
 /* Plain device memory for callers without a CUDA runtime of their own. */
 eh_status eh_device_alloc(eh_context* ctx, uint64_t bytes, void** out);
