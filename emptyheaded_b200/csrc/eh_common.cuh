@@ -205,6 +205,11 @@ void radix_sort_u64(uint64_t* keys, uint64_t* tmp, uint64_t n, int bits, cudaStr
 // The same with a uint32 payload per key, stable (vtmp holds n values).
 void radix_sort_kv(uint64_t* keys, uint64_t* ktmp, uint32_t* vals, uint32_t* vtmp, uint64_t n, int bits,
                    cudaStream_t s);
+// Stable order of uint32 payloads by 32-bit keys (low `bits` bits): returns
+// the buffer, vals or vtmp, that holds the payloads in key order; the keys
+// are not kept (no key writes on the last pass, no copy back).
+uint32_t* radix_sort_payload_u32(uint32_t* keys, uint32_t* ktmp, uint32_t* vals, uint32_t* vtmp, uint64_t n, int bits,
+                                 cudaStream_t s);
 
 // Keep the first of each run of equal keys (keys sorted).  Writes the
 // compacted keys to out and the count to *count_host (synchronises).

@@ -144,7 +144,8 @@ constexpr int kSortRounds = 16;
 constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096 keys
 constexpr int kRadix = 256;
 
-__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint64_t* __restrict__ keys, uint64_t n,
+template <typename K>
+__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const K* __restrict__ keys, uint64_t n,
                                                                   int shift, uint32_t* __restrict__ counts,
                                                                   uint32_t tiles) {
   __shared__ uint32_t h[kRadix];
@@ -164,20 +165,23 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint64_t
 // placed in digit order in shared memory (stable: tile digit start + the
 // warp's offset within the digit + the key's rank in its warp), then written
 // out in that order, so consecutive threads write consecutive slots of one
-// digit's run (coalesced) instead of 256 scattered runs per round.
-template <bool kVals>
-__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint64_t* __restrict__ keys,
-                                                                     uint64_t* __restrict__ out, uint64_t n,
+// digit's run (coalesced) instead of 256 scattered runs per round.  With
+// write_keys = 0 only the payloads are written (the last pass of a sort whose
+// caller reads the payloads alone).
+template <typename K, bool kVals>
+__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const K* __restrict__ keys,
+                                                                     K* __restrict__ out, uint64_t n,
                                                                      int shift,
                                                                      const uint32_t* __restrict__ offsets,
                                                                      uint32_t tiles,
                                                                      const uint32_t* __restrict__ vin,
-                                                                     uint32_t* __restrict__ vout) {
+                                                                     uint32_t* __restrict__ vout, int write_keys) {
   __shared__ uint32_t whist[kSortWarps][kRadix];
   __shared__ uint32_t tile_off[kRadix];
   __shared__ uint32_t tstart[kRadix];
   __shared__ uint32_t wtot[kSortWarps];
-  extern __shared__ uint64_t skeys[];  // kSortTile keys, then (kVals) kSortTile uint32 payloads
+  extern __shared__ __align__(16) unsigned char sort_smem[];  // kSortTile keys, then (kVals) kSortTile payloads
+  K* skeys = reinterpret_cast<K*>(sort_smem);
   uint32_t* svals = reinterpret_cast<uint32_t*>(skeys + kSortTile);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&whist[0][0])[i] = 0;
@@ -186,7 +190,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint6
   // warp w owns keys [base + w*512, base + (w+1)*512), round-major
   const uint64_t tbase = (uint64_t)blockIdx.x * kSortTile;
   const uint64_t wbase = tbase + (uint64_t)wid * (32 * kSortRounds);
-  uint64_t k[kSortRounds];
+  K k[kSortRounds];
   uint32_t pos[kSortRounds];
   const uint32_t lt = lanemask_lt();
 #pragma unroll
@@ -235,62 +239,82 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint6
   __syncthreads();
   const uint32_t cnt = (uint32_t)min((uint64_t)kSortTile, n - tbase);
   for (uint32_t j = threadIdx.x; j < cnt; j += kSortThreads) {
-    const uint64_t key = skeys[j];
+    const K key = skeys[j];
     const uint32_t d = (uint32_t)((key >> shift) & 0xff);
     const uint32_t dst = tile_off[d] + (j - tstart[d]);
-    out[dst] = key;
+    if (write_keys) out[dst] = key;
     if (kVals) vout[dst] = svals[j];
   }
 }
 
-static size_t scatter_smem(bool vals) { return (size_t)kSortTile * (8 + (vals ? 4 : 0)); }
+template <typename K>
+static size_t scatter_smem(bool vals) {
+  return (size_t)kSortTile * (sizeof(K) + (vals ? 4 : 0));
+}
 
-// LSD passes; with vals != nullptr a uint32 payload follows its key (stable)
-static void radix_sort_impl(uint64_t* keys, uint64_t* tmp, uint32_t* vals, uint32_t* vtmp, uint64_t n, int bits,
-                            cudaStream_t s) {
-  if (n < 2) return;
+template <typename K>
+static void set_scatter_smem() {
+  static bool done = false;  // the staged scatter takes more than the default 48 KB
+  if (done) return;
+  EH_CUDA(cudaFuncSetAttribute(radix_scatter_kernel<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)scatter_smem<K>(true)));
+  EH_CUDA(cudaFuncSetAttribute(radix_scatter_kernel<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)scatter_smem<K>(false)));
+  done = true;
+}
+
+// LSD passes; with vals != nullptr a uint32 payload follows its key
+// (stable).  copy_back: the sorted keys (and payloads) end in keys / vals;
+// otherwise only the payloads are produced, in the buffer returned (vals or
+// vtmp), and the keys are left unspecified.
+template <typename K>
+static uint32_t* radix_sort_impl(K* keys, K* tmp, uint32_t* vals, uint32_t* vtmp, uint64_t n, int bits,
+                                 bool copy_back, cudaStream_t s) {
+  if (n < 2) return vals;
   EH_REQUIRE(n < (1ull << 32), EH_ERR_UNSUPPORTED, "radix sort supports fewer than 2^32 keys");
   const uint32_t tiles = (uint32_t)((n + kSortTile - 1) / kSortTile);
   DevBuf<uint32_t> counts((uint64_t)kRadix * tiles, s);
-  static bool smem_set = false;  // the staged scatter takes more than the default 48 KB
-  if (!smem_set) {
-    EH_CUDA(cudaFuncSetAttribute(radix_scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)scatter_smem(true)));
-    EH_CUDA(cudaFuncSetAttribute(radix_scatter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)scatter_smem(false)));
-    smem_set = true;
-  }
-  uint64_t* src = keys;
-  uint64_t* dst = tmp;
+  set_scatter_smem<K>();
+  K* src = keys;
+  K* dst = tmp;
   uint32_t* vsrc = vals;
   uint32_t* vdst = vtmp;
   for (int shift = 0; shift < bits; shift += 8) {
-    radix_hist_kernel<<<tiles, kSortThreads, 0, s>>>(src, n, shift, counts.p, tiles);
+    const int write_keys = copy_back || shift + 8 < bits;
+    radix_hist_kernel<K><<<tiles, kSortThreads, 0, s>>>(src, n, shift, counts.p, tiles);
     EH_CHECK_LAUNCH();
     exclusive_scan<uint32_t>(counts.p, counts.p, (uint64_t)kRadix * tiles, nullptr, s);
     if (vals)
-      radix_scatter_kernel<true><<<tiles, kSortThreads, scatter_smem(true), s>>>(src, dst, n, shift, counts.p, tiles,
-                                                                                vsrc, vdst);
+      radix_scatter_kernel<K, true><<<tiles, kSortThreads, scatter_smem<K>(true), s>>>(
+          src, dst, n, shift, counts.p, tiles, vsrc, vdst, write_keys);
     else
-      radix_scatter_kernel<false><<<tiles, kSortThreads, scatter_smem(false), s>>>(src, dst, n, shift, counts.p,
-                                                                                  tiles, nullptr, nullptr);
+      radix_scatter_kernel<K, false><<<tiles, kSortThreads, scatter_smem<K>(false), s>>>(
+          src, dst, n, shift, counts.p, tiles, nullptr, nullptr, write_keys);
     EH_CHECK_LAUNCH();
     std::swap(src, dst);
     std::swap(vsrc, vdst);
   }
-  if (src != keys) {
-    EH_CUDA(cudaMemcpyAsync(keys, src, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+  if (copy_back && src != keys) {
+    EH_CUDA(cudaMemcpyAsync(keys, src, n * sizeof(K), cudaMemcpyDeviceToDevice, s));
     if (vals) EH_CUDA(cudaMemcpyAsync(vals, vsrc, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    return vals;
   }
+  return vsrc;
 }
 
 void radix_sort_u64(uint64_t* keys, uint64_t* tmp, uint64_t n, int bits, cudaStream_t s) {
-  radix_sort_impl(keys, tmp, nullptr, nullptr, n, bits, s);
+  radix_sort_impl<uint64_t>(keys, tmp, nullptr, nullptr, n, bits, true, s);
 }
 
 void radix_sort_kv(uint64_t* keys, uint64_t* ktmp, uint32_t* vals, uint32_t* vtmp, uint64_t n, int bits,
                    cudaStream_t s) {
-  radix_sort_impl(keys, ktmp, vals, vtmp, n, bits, s);
+  radix_sort_impl<uint64_t>(keys, ktmp, vals, vtmp, n, bits, true, s);
+}
+
+uint32_t* radix_sort_payload_u32(uint32_t* keys, uint32_t* ktmp, uint32_t* vals, uint32_t* vtmp, uint64_t n, int bits,
+                                 cudaStream_t s) {
+  EH_REQUIRE(bits >= 1 && bits <= 32, EH_ERR_INVALID, "32-bit keys sort on 1 to 32 bits");
+  return radix_sort_impl<uint32_t>(keys, ktmp, vals, vtmp, n, bits, false, s);
 }
 
 // ================================================================ unique

@@ -645,8 +645,8 @@ __device__ __forceinline__ void rev_range(int dir, uint64_t e, uint64_t a_lo, ui
 // key = head position of b (sentinel for rows the plans never read),
 // payload = the row; rows arrive in row order, so a stable sort on the key
 // alone leaves each b's rows in row order
-__global__ void rev_key_kernel(TrieView t, const uint32_t* __restrict__ seg, int dir, uint64_t sentinel,
-                               uint64_t* __restrict__ keys, uint32_t* __restrict__ rowid, uint32_t* __restrict__ cnt) {
+__global__ void rev_key_kernel(TrieView t, const uint32_t* __restrict__ seg, int dir, uint32_t sentinel,
+                               uint32_t* __restrict__ keys, uint32_t* __restrict__ rowid, uint32_t* __restrict__ cnt) {
   for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < t.rows; e += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t ha = seg[e];
     const uint32_t a = t.head[ha], b = t.vals[e];
@@ -654,7 +654,7 @@ __global__ void rev_key_kernel(TrieView t, const uint32_t* __restrict__ seg, int
     uint64_t lo, hi;
     rev_range(dir, e, t.off[ha], t.off[ha + 1], lo, hi);
     const bool keep = hb >= 0 && hi > lo && (dir != DIR_SYM || a < b);
-    keys[e] = keep ? (uint64_t)hb : sentinel;
+    keys[e] = keep ? (uint32_t)hb : sentinel;
     rowid[e] = (uint32_t)e;
     if (keep) atomicAdd(&cnt[hb], 1u);
   }
@@ -723,10 +723,11 @@ void trie_build_reverse(eh_context* ctx, eh_trie* t) {
     t->dir = (c[2] == 0 && c[3] == 0) ? DIR_SYM : DIR_GENERAL;
   }
   ph_dir.end();
-  // group the rows a->b the plans read by b (stable: row order within b)
+  // group the rows a->b the plans read by b (stable: row order within b);
+  // head positions are below 2^32, so 32-bit keys on bits_for(n_head) bits
   const int bh = bits_for(t->n_head);
-  const uint64_t sentinel = (1ull << bh) - 1;  // above every head position
-  DevBuf<uint64_t> keys(t->rows, s), ktmp(t->rows, s);
+  const uint32_t sentinel = (uint32_t)((1ull << bh) - 1);  // above every head position
+  DevBuf<uint32_t> keys(t->rows, s), ktmp(t->rows, s);
   DevBuf<uint32_t> rowid(t->rows, s), vtmp(t->rows, s);
   DevBuf<uint32_t> per(t->n_head + 1, s);
   EH_CUDA(cudaMemsetAsync(per.p, 0, (t->n_head + 1) * 4, s));
@@ -735,12 +736,16 @@ void trie_build_reverse(eh_context* ctx, eh_trie* t) {
   EH_CHECK_LAUNCH();
   ph_key.end();
   TracePhase ph_sort("reverse.sort", s);
-  radix_sort_kv(keys.p, ktmp.p, rowid.p, vtmp.p, t->rows, bh, s);
-  // only the sorted row ids are read from here on: hand the sort's 1.3 GB
-  // (at R-MAT-22) back to the pool before the reverse arrays are allocated
+  const uint32_t* sorted = radix_sort_payload_u32(keys.p, ktmp.p, rowid.p, vtmp.p, t->rows, bh, s);
+  // only the sorted row ids are read from here on: hand the sort's other
+  // buffers (768 MB at R-MAT-22) back to the pool before the reverse arrays
+  // are allocated
   keys.release();
   ktmp.release();
-  vtmp.release();
+  if (sorted == rowid.p)
+    vtmp.release();
+  else
+    rowid.release();
   ph_sort.end();
   TracePhase ph_fill("reverse.offsets+fill", s);
   {
@@ -761,7 +766,7 @@ void trie_build_reverse(eh_context* ctx, eh_trie* t) {
   t->rev_wpre.alloc(n + 1, s);
   EH_CUDA(cudaMemsetAsync(t->rev_wpre.p, 0, (n + 1) * 8, s));
   if (n) {
-    rev_fill_kernel<<<grid, 256, 0, s>>>(t->view(), seg.p, t->dir, rowid.p, n, t->rev_lo.p, t->rev_hi.p,
+    rev_fill_kernel<<<grid, 256, 0, s>>>(t->view(), seg.p, t->dir, sorted, n, t->rev_lo.p, t->rev_hi.p,
                                          t->rev_src.p, t->rev_wpre.p);
     EH_CHECK_LAUNCH();
     exclusive_scan<uint64_t>(t->rev_wpre.p, t->rev_wpre.p, n, t->rev_wpre.p + n, s);
