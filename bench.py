@@ -299,6 +299,8 @@ def ours_arm(args):
     ms_l = rmax(statistics.mean(ql))
     kern_l = rmax(statistics.mean(kl))
     kern_h = rmax(statistics.mean(kh))
+    med_h = rmax(statistics.median(qh))
+    med_l = rmax(statistics.median(ql))
 
     # ---- e2e through the host-buffer entry: CSR in pinned host memory,
     # copied to the device every step (plus the trie index build), count back
@@ -361,6 +363,7 @@ def ours_arm(args):
             "config": {"workload": WORKLOAD, "rows": info_h["rows"], "nodes": nodes, "layout": "learned",
                        "heuristic_ms": ms_h, "learned_ms": ms_l, "learned_speedup": ms_h / ms_l,
                        "heuristic_kernel_ms": kern_h, "learned_kernel_ms": kern_l,
+                       "heuristic_median_ms": med_h, "learned_median_ms": med_l,
                        "l2": "trie (%.2f GB) larger than L2, and a 256 MB buffer written between steps"
                              % (info_h["device_bytes"] / 1e9),
                        "trie_build_s": build_s, "parallelism": "shards of work items" if world > 1 else "single GPU",
