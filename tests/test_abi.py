@@ -41,5 +41,8 @@ def test_null_arguments_are_rejected(eh):
     assert L.eh_context_create(0, None) == 1
     assert L.eh_trie_info_get(None, None) == 1
     assert b"null" in L.eh_last_error()
+    assert L.eh_context_memory(None, None, None, None) == 1
+    assert L.eh_context_reserve(None, 1 << 20) == 1
+    assert b"null" in L.eh_last_error()
     assert L.eh_trie_free(None) == 0
     assert L.eh_context_destroy(None) == 0
