@@ -157,16 +157,48 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """Per-launch DRAM bytes (read + write) of the intersection kernel from
-    the committed one-pass ncu capture at this workload
-    (profiles/triangle_kernel_rmat22_dram.json), if present."""
-    p = os.path.join(ROOT, "profiles", "triangle_kernel_rmat22_dram.json")
+def profile_record(layout):
+    """Per-launch ncu figures of the intersection kernel at this workload for
+    one layout policy (profiles/triangle_kernel_rmat22_<layout>_dram.json,
+    written from a one-pass capture; see the .md beside it), or None."""
+    p = os.path.join(ROOT, "profiles", "triangle_kernel_rmat22_%s_dram.json" % layout)
     if os.path.exists(p):
         with open(p) as f:
-            d = json.load(f)
-        return int(d["dram_bytes_read"]) + int(d["dram_bytes_write"])
+            return json.load(f)
     return None
+
+
+def roofline(kernel_ms, alg_bytes, wedges, layout, peak, peak_kind, sm_mhz):
+    """HBM roofline of the timed intersection kernel.  frac is measured DRAM
+    traffic (ncu, same kernel, same layouts, per launch) over the kernel's
+    CUDA-event time, against the measured copy peak.  The algorithmic bytes
+    (both uint32 inputs of every pairwise intersection the reference loop
+    nest evaluates) are reported beside it: most of them are served from
+    shared memory and L2, so their rate is not a DRAM figure.  The issue
+    side (warp instructions against 4 per SM per cycle) is what bounds this
+    kernel."""
+    rec = profile_record(layout)
+    sec = kernel_ms * 1e-3
+    out = {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
+           "kernel": "eh::triangle_kernel<0> (MODE_COUNT)",
+           "algorithmic_bytes": alg_bytes, "algorithmic_gbs": alg_bytes / sec / 1e9,
+           "alg_over_peak": alg_bytes / sec / 1e9 / peak}
+    if rec:
+        traffic = int(rec["dram_bytes_read"]) + int(rec["dram_bytes_write"])
+        out.update({"achieved": traffic / sec / 1e9, "frac": traffic / sec / 1e9 / peak, "traffic": traffic,
+                    "traffic_source": "profiles/triangle_kernel_rmat22_%s_dram.json" % layout})
+        inst = rec.get("warp_instructions")
+        if inst:
+            sms = int(rec.get("sms", 148))
+            mhz = sm_mhz or float(rec.get("sm_mhz", 1965.0))
+            issue_peak = 4.0 * sms * mhz * 1e6 * sec  # one warp instruction per SMSP per cycle
+            out["issue"] = {"warp_instructions": int(inst), "per_candidate": int(inst) / max(1, wedges),
+                            "issue_frac": int(inst) / issue_peak, "sm_mhz": mhz,
+                            "note": "warp instructions per launch from the same capture; peak = 4 per SM per cycle"}
+    else:
+        out.update({"achieved": None, "frac": None, "traffic": None,
+                    "traffic_source": "no capture of this kernel with %s layouts in profiles/" % layout})
+    return out
 
 
 def train_layout_model(E, trie, steps_per_layout=1):
@@ -353,9 +385,9 @@ def ours_arm(args):
 
     if rank == 0:
         peak, peak_kind = load_peaks()
-        alg = st_l["algorithmic_bytes"]
-        achieved = alg / (kern_l * 1e-3) / 1e9
-        traffic = profile_traffic()
+        layout_name = "learned" if "error" not in learn_info else "heuristic"
+        roof = roofline(kern_l, st_l["algorithmic_bytes"], st_l["wedges"], layout_name, peak,
+                        peak_kind + " (hbm_gbs)", clocks.get("sm_mhz"))
         line = {
             "metric": METRIC, "value": ms_l, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_l, "higher_is_better": False, "scaling": "strong",
@@ -370,9 +402,7 @@ def ours_arm(args):
                        "schedule_heuristic": cfg_h, "schedule_learned": cfg_l,
                        "learned": learn_info},
             "count": g["triangle"],
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_kind": peak_kind + " (hbm_gbs)",
-                         "algorithmic_bytes": alg, "kernel": "eh::triangle_kernel<false>"},
+            "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(ll / max(1, args.steps)) * args.steps,
@@ -385,6 +415,41 @@ def ours_arm(args):
     return 0
 
 
+def case_arm(args):
+    """A small self-checking query case for profiler captures (not a bench
+    line): builds the R-MAT trie of --scale on the device, lays it out with
+    --layout (learned: the cost model is trained on this trie first), and
+    runs the query --repeat times inside the NVTX range "case", printing the
+    counts and device times.  Captures select the case's launches with
+    --nvtx --nvtx-include "case/"."""
+    import torch
+    import emptyheaded_b200 as E
+    from emptyheaded_b200 import learn, workloads as W
+
+    t = W.build_rmat_trie(E, args.scale, SEED)
+    forced = {"uint": E.UINTEGER, "bitset": E.RANGE_BITSET, "block": E.BLOCK_BITSET}
+    learn_info = None
+    if args.layout == "learned":
+        model, learn_info = learn.train_from_trie(E, t)
+        t.relayout(policy=E.LEARNED, model=model)
+    elif args.layout in forced:
+        t.relayout(policy=E.FORCED, forced=forced[args.layout], max_bitset_bytes=1 << 50)
+    runs = []
+    t.count(args.query)  # warm
+    torch.cuda.nvtx.range_push("case")
+    for _ in range(args.repeat):
+        c, st = t.count(args.query, stats=True)
+        runs.append({"count": c, "query_ms": st["query_ms"], "kernel_ms": st["kernel_ms"], "wedges": st["wedges"],
+                     "algorithmic_bytes": st["algorithmic_bytes"]})
+    torch.cuda.nvtx.range_pop()
+    g = W.golden_counts().get("rmat_s%d_ef16_s%d" % (args.scale, SEED), {})
+    ok = all(r["count"] == g[args.query] for r in runs) if args.query in g else None
+    print(json.dumps({"case": "rmat%d" % args.scale, "query": args.query, "layout": args.layout, "ok": ok,
+                      "info": t.info(), "learned": learn_info, "runs": runs}))
+    t.free()
+    return 0 if ok in (None, True) else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -392,7 +457,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--case", action="store_true", help="profiler case instead of the bench line")
+    ap.add_argument("--scale", type=int, default=20, help="--case: R-MAT scale")
+    ap.add_argument("--layout", default="heuristic", choices=["heuristic", "learned", "uint", "bitset", "block"],
+                    help="--case: layout policy")
+    ap.add_argument("--query", default="triangle", help="--case: query")
+    ap.add_argument("--repeat", type=int, default=2, help="--case: runs inside the NVTX range")
     args = ap.parse_args()
+    if args.case:
+        return case_arm(args)
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return reference_arm(args)

@@ -29,7 +29,7 @@ LIB_PATH = os.environ.get("EH_B200_LIB") or os.path.join(_HERE, "_lib", "libeh_b
 
 # status codes and enums (include/eh_b200.h)
 EH_OK = 0
-STATUS_NAMES = {1: "INVALID", 2: "CUDA", 3: "OOM", 4: "TIMEOUT", 5: "UNSUPPORTED", 6: "IO", 7: "NO_DEVICE"}
+STATUS_NAMES = {1: "INVALID", 2: "CUDA", 3: "OOM", 5: "UNSUPPORTED", 6: "IO", 7: "NO_DEVICE"}
 RANGE_BITSET, UINTEGER, BLOCK_BITSET = 0, 1, 3
 HEURISTIC, LEARNED, FORCED = 0, 1, 2
 QUERIES = {"triangle": 0, "clique4": 1, "lollipop": 2, "barbell": 3}
@@ -59,7 +59,7 @@ class TrieInfo(ctypes.Structure):
 
 class ExecConfig(ctypes.Structure):
     _fields_ = [("warps_per_block", ctypes.c_int), ("chunk_pairs", ctypes.c_int), ("long_row", ctypes.c_int),
-                ("smem_words", ctypes.c_int), ("record_timings", ctypes.c_int), ("spin_limit", ctypes.c_uint64),
+                ("smem_words", ctypes.c_int), ("record_timings", ctypes.c_int),
                 ("shard_index", ctypes.c_int), ("shard_count", ctypes.c_int)]
 
 
@@ -75,7 +75,7 @@ class Rule(ctypes.Structure):
 class QueryStats(ctypes.Structure):
     _fields_ = [("query_ms", ctypes.c_float), ("kernel_ms", ctypes.c_float), ("launches", ctypes.c_uint32),
                 ("work_items", ctypes.c_uint64), ("wedges", ctypes.c_uint64),
-                ("algorithmic_bytes", ctypes.c_uint64), ("timed_out", ctypes.c_int)]
+                ("algorithmic_bytes", ctypes.c_uint64)]
 
 
 _lib = None
@@ -141,6 +141,7 @@ def lib():
             "eh_query_count_batched": [_P, _P, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ExecConfig), _P,
                                        ctypes.POINTER(QueryStats)],
             "eh_triangle_annotation": [_P, _P, ctypes.POINTER(ExecConfig), _P],
+            "eh_query_weighted_root": [_P, _P, ctypes.c_int, _P, ctypes.c_uint32, _u64p],
             "eh_batch_create": [_P, _P, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ExecConfig),
                                 ctypes.POINTER(_P)],
             "eh_batch_run": [_P, _P, _P, ctypes.POINTER(QueryStats)],
@@ -320,7 +321,6 @@ def _exec_cfg(warps=0, chunk=0, smem_words=0, record=False, shard=(0, 1), long_r
     e.long_row = long_row
     e.smem_words = smem_words
     e.record_timings = 1 if record else 0
-    e.spin_limit = 0
     e.shard_index, e.shard_count = shard
     return e
 
@@ -464,6 +464,16 @@ class Trie:
                                           _ptr(b), _ptr(c), rows, ctypes.byref(n)))
         out = [a[:rows], b[:rows]] + ([] if project else [c[:rows]])
         return np.stack(out, 1)
+
+    def weighted_root(self, query, z):
+        """Root bag of lollipop / barbell over an annotation z given by node
+        value (eh_query_weighted_root): lollipop sum_a z(a)|N(a)|, barbell
+        sum over rows (a,x) of z(a)z(x), modulo 2^64."""
+        z = np.ascontiguousarray(z, np.uint64)
+        r = ctypes.c_uint64()
+        _check(lib().eh_query_weighted_root(self.ctx.h, self.h, QUERIES[query], _ptr(z) if len(z) else None, len(z),
+                                            ctypes.byref(r)))
+        return r.value
 
     def triangle_annotation(self):
         nh = self.info()["n_head"]

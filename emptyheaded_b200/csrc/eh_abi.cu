@@ -625,6 +625,15 @@ eh_status eh_triangle_annotation(eh_context* ctx, const eh_trie* trie, const eh_
   });
 }
 
+eh_status eh_query_weighted_root(eh_context* ctx, const eh_trie* trie, int query, const uint64_t* z,
+                                 uint32_t n_values, uint64_t* result) {
+  return guarded([&] {
+    need(ctx && trie && result, "null argument");
+    set_device(ctx);
+    query_weighted_root(ctx, trie, query, z, n_values, result);
+  });
+}
+
 eh_status eh_query_count_host_csr(eh_context* ctx, const uint32_t* head, uint32_t n_head, const uint64_t* off,
                                   const uint32_t* vals, uint32_t n_nodes, const eh_layout_config* cfg, int query,
                                   const eh_exec_config* ecfg, uint64_t* result, eh_query_stats* stats) {

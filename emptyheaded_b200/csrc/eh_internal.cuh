@@ -151,6 +151,8 @@ void query_count(eh_context* ctx, const eh_trie* t, int query, const eh_exec_con
 void query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query,
                          const eh_exec_config* cfg, uint64_t* results, eh_query_stats* stats);
 void triangle_annotation(eh_context* ctx, const eh_trie* t, const eh_exec_config* cfg, uint64_t* annot_dev);
+void query_weighted_root(eh_context* ctx, const eh_trie* t, int query, const uint64_t* z, uint32_t n_values,
+                         uint64_t* result);
 void query_count_select(eh_context* ctx, const eh_trie* t, int query, uint32_t value, const eh_exec_config* cfg,
                         uint64_t* result, eh_query_stats* stats);
 eh_batch* batch_create(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query,

@@ -57,11 +57,17 @@ extern "C" eh_status eh_query_count_noalloc(eh_context* ctx, const eh_trie* trie
                                             const eh_exec_config* cfg, uint64_t* result) {
   try {
     if (!ctx || !trie || !result) throw eh::Error{EH_ERR_INVALID, "null argument"};
-    EH_CUDA(cudaSetDevice(ctx->device));
     if (ctx->device < 0 || ctx->device >= kMaxDevices) throw eh::Error{EH_ERR_UNSUPPORTED, "device index too large"};
+    EH_CUDA(cudaSetDevice(ctx->device));
     std::lock_guard<std::mutex> lk(g_device_mu[ctx->device]);
-    unsigned char* scratch = scratch_for(ctx->device);
-    eh::query_count_in_scratch(ctx, trie, query, cfg, scratch, EH_NOALLOC_SCRATCH_BYTES, result);
+    try {
+      unsigned char* scratch = scratch_for(ctx->device);
+      eh::query_count_in_scratch(ctx, trie, query, cfg, scratch, EH_NOALLOC_SCRATCH_BYTES, result);
+    } catch (...) {
+      // a failed call releases the lock only once its own GPU work is done
+      cudaStreamSynchronize(ctx->stream);
+      throw;
+    }
     return EH_OK;
   } catch (const eh::Error& e) {
     eh::set_error(e.msg);

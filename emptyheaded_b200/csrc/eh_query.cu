@@ -528,7 +528,6 @@ struct QueryOut {
   unsigned long long* annot;   // per head entry annotation or null
   float* records;              // per item timing records or null
   unsigned int* queue;         // atomic queue head
-  unsigned int* error;         // set when a bound is hit
   unsigned long long* item_counts;  // per item count x count_mult (materialize sizing) or null
   uint32_t count_mult;
   const unsigned long long* item_off;  // MODE_MAT: first output row of each item
@@ -1005,7 +1004,7 @@ static void launch(eh_context* ctx, Prepared& P, unsigned long long* d_total, un
   if (!P.n_items) return;
   EH_CUDA(cudaMemsetAsync(P.q.p, 0, 8, s));
   const ExecParams& ep = P.ep;
-  QueryOut out{ep.shard_index, ep.shard_count, ep.long_row, d_total, d_annot, d_records, P.q.p, P.q.p + 1};
+  QueryOut out{ep.shard_index, ep.shard_count, ep.long_row, d_total, d_annot, d_records, P.q.p};
   out.sel = P.sel;
   for (int k = 0; k < kHot; k++) out.hot[k] = P.hot[k];
   out.gsbuf = ep.s_cap ? P.gs.p : nullptr;
@@ -1070,7 +1069,101 @@ static void fill_stats(eh_query_stats* st, float query_ms, const Launch& L, uint
   st->work_items = items;
   st->wedges = pairs;
   st->algorithmic_bytes = alg;
-  st->timed_out = 0;
+}
+
+// The root bag of the lollipop / barbell plans over a per-head-entry
+// annotation T (the annotated bag's z, by head position of t; Tv: the same
+// by node value, or null to derive it): LollipopAgg sum_a T(a) * |N(a)|,
+// BarbellAgg sum_a T(a) * sum_{x in N(a)} Tv(x).  Adds into total[0];
+// returns the kernels launched.
+static uint32_t root_bag(eh_context* ctx, const eh_trie* t, int query, const unsigned long long* T,
+                         const unsigned long long* Tv, unsigned long long* total) {
+  cudaStream_t s = ctx->stream;
+  if (!t->n_head) return 0;
+  uint32_t launches = 0;
+  if (query == EH_QUERY_LOLLIPOP) {
+    root_kernel<false><<<num_sms() * 8, 256, 0, s>>>(t->view(), T, nullptr, total);
+    EH_CHECK_LAUNCH();
+    return 1;
+  }
+  DevBuf<unsigned long long> tv;
+  if (!Tv) {
+    tv.alloc(t->n_nodes ? t->n_nodes : 1, s);
+    t_by_value_kernel<<<num_sms() * 8, 256, 0, s>>>(t->view(), T, tv.p);
+    EH_CHECK_LAUNCH();
+    Tv = tv.p;
+    launches++;
+  }
+  root_kernel<true><<<num_sms() * 8, 256, 0, s>>>(t->view(), T, Tv, total);
+  EH_CHECK_LAUNCH();
+  launches++;
+  if (t->info.max_set > kRootBig) {
+    DevBuf<uint32_t> idx(t->n_head, s);
+    DevBuf<unsigned int> nb(1, s);
+    EH_CUDA(cudaMemsetAsync(nb.p, 0, 4, s));
+    root_big_sets_kernel<<<num_sms() * 4, 256, 0, s>>>(t->view(), idx.p, nb.p);
+    EH_CHECK_LAUNCH();
+    unsigned int hn = 0;
+    EH_CUDA(cudaMemcpyAsync(&hn, nb.p, 4, cudaMemcpyDeviceToHost, s));
+    EH_CUDA(cudaStreamSynchronize(s));
+    std::vector<uint32_t> big(hn);
+    if (hn) EH_CUDA(cudaMemcpyAsync(big.data(), idx.p, 4ull * hn, cudaMemcpyDeviceToHost, s));
+    EH_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t a : big) {
+      root_big_kernel<<<num_sms() * 4, 256, 0, s>>>(t->view(), a, T, Tv, total);
+      EH_CHECK_LAUNCH();
+    }
+    launches += 1 + hn;
+  }
+  return launches;
+}
+
+// z by node value (zero beyond n_values) -> the same by head position
+__global__ void z_by_head_kernel(TrieView t, const unsigned long long* __restrict__ zv, uint32_t n_values,
+                                 unsigned long long* __restrict__ T) {
+  for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < t.n_head; a += gridDim.x * blockDim.x) {
+    const uint32_t v = t.head[a];
+    T[a] = v < n_values ? zv[v] : 0ull;
+  }
+}
+
+// The root bag of lollipop / barbell over an annotation z given by value on
+// the host (the generated root bags of an annotated intermediate,
+// EHGenerator.scala:399-480 with TrieIterator::get_annotation,
+// TrieIterator.cpp:45-59): LOLLIPOP sum_a z(a) |N(a)|, BARBELL
+// sum_{(a,x)} z(a) z(x), modulo 2^64.
+void query_weighted_root(eh_context* ctx, const eh_trie* t, int query, const uint64_t* z, uint32_t n_values,
+                         uint64_t* result) {
+  cudaStream_t s = ctx->stream;
+  EH_REQUIRE(query == EH_QUERY_LOLLIPOP || query == EH_QUERY_BARBELL, EH_ERR_INVALID,
+             "the weighted root bag is EH_QUERY_LOLLIPOP or EH_QUERY_BARBELL");
+  EH_REQUIRE(t->ctx == ctx, EH_ERR_INVALID, "trie belongs to another context");
+  EH_REQUIRE(n_values == 0 || z, EH_ERR_INVALID, "null annotation");
+  const uint32_t nv = std::min(n_values, t->n_nodes);
+  DevBuf<unsigned long long> zv(nv ? nv : 1, s), T(t->n_head ? t->n_head : 1, s), total(1, s);
+  EH_CUDA(cudaMemsetAsync(total.p, 0, 8, s));
+  if (nv) EH_CUDA(cudaMemcpyAsync(zv.p, z, 8ull * nv, cudaMemcpyHostToDevice, s));
+  if (t->n_head) {
+    z_by_head_kernel<<<num_sms() * 4, 256, 0, s>>>(t->view(), zv.p, nv, T.p);
+    EH_CHECK_LAUNCH();
+    if (query == EH_QUERY_BARBELL) {
+      // Tv over the whole value domain: values of the relation outside its head still carry z
+      DevBuf<unsigned long long> tv(t->n_nodes ? t->n_nodes : 1, s);
+      EH_CUDA(cudaMemsetAsync(tv.p, 0, (size_t)(t->n_nodes ? t->n_nodes : 1) * 8, s));
+      if (nv) EH_CUDA(cudaMemcpyAsync(tv.p, zv.p, 8ull * nv, cudaMemcpyDeviceToDevice, s));
+      root_bag(ctx, t, query, T.p, tv.p, total.p);
+      unsigned long long h = 0;
+      EH_CUDA(cudaMemcpyAsync(&h, total.p, 8, cudaMemcpyDeviceToHost, s));
+      EH_CUDA(cudaStreamSynchronize(s));
+      *result = h;
+      return;
+    }
+    root_bag(ctx, t, query, T.p, nullptr, total.p);
+  }
+  unsigned long long h = 0;
+  EH_CUDA(cudaMemcpyAsync(&h, total.p, 8, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaStreamSynchronize(s));
+  *result = h;
 }
 
 void query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query,
@@ -1118,37 +1211,7 @@ void query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t 
     EH_CUDA(cudaMemsetAsync(T.p, 0, (t->n_head ? t->n_head : 1) * 8, s));
     EH_CUDA(cudaMemsetAsync(dummy.p, 0, 8, s));
     L = run_plans(ctx, tries, 1, EH_QUERY_TRIANGLE, ep, true, dummy.p, T.p, nullptr, &items, &pairs);
-    if (t->n_head) {
-      if (query == EH_QUERY_LOLLIPOP) {
-        root_kernel<false><<<num_sms() * 8, 256, 0, s>>>(t->view(), T.p, nullptr, total.p);
-      } else {
-        DevBuf<unsigned long long> Tv(t->n_nodes ? t->n_nodes : 1, s);
-        t_by_value_kernel<<<num_sms() * 8, 256, 0, s>>>(t->view(), T.p, Tv.p);
-        root_kernel<true><<<num_sms() * 8, 256, 0, s>>>(t->view(), T.p, Tv.p, total.p);
-        EH_CHECK_LAUNCH();
-        L.launches++;
-        if (t->info.max_set > kRootBig) {
-          DevBuf<uint32_t> idx(t->n_head, s);
-          DevBuf<unsigned int> nb(1, s);
-          EH_CUDA(cudaMemsetAsync(nb.p, 0, 4, s));
-          root_big_sets_kernel<<<num_sms() * 4, 256, 0, s>>>(t->view(), idx.p, nb.p);
-          EH_CHECK_LAUNCH();
-          unsigned int hn = 0;
-          EH_CUDA(cudaMemcpyAsync(&hn, nb.p, 4, cudaMemcpyDeviceToHost, s));
-          EH_CUDA(cudaStreamSynchronize(s));
-          std::vector<uint32_t> big(hn);
-          if (hn) EH_CUDA(cudaMemcpyAsync(big.data(), idx.p, 4ull * hn, cudaMemcpyDeviceToHost, s));
-          EH_CUDA(cudaStreamSynchronize(s));
-          for (uint32_t a : big) {
-            root_big_kernel<<<num_sms() * 4, 256, 0, s>>>(t->view(), a, T.p, Tv.p, total.p);
-            EH_CHECK_LAUNCH();
-          }
-          L.launches += 1 + hn;
-        }
-      }
-      EH_CHECK_LAUNCH();
-      L.launches++;
-    }
+    L.launches += root_bag(ctx, t, query, T.p, nullptr, total.p);
   }
   std::vector<unsigned long long> h(n);
   EH_CUDA(cudaMemcpyAsync(h.data(), total.p, n * 8, cudaMemcpyDeviceToHost, s));
@@ -1444,7 +1507,7 @@ void query_materialize(eh_context* ctx, const eh_trie* t, int query, const eh_ex
       total(1, s), rows(1, s);
   EH_CUDA(cudaMemsetAsync(total.p, 0, 8, s));
   const uint32_t mult = t->dir == DIR_SYM ? 6u : 1u;
-  QueryOut out{0, 1, P.ep.long_row, total.p, nullptr, nullptr, P.q.p, P.q.p + 1};
+  QueryOut out{0, 1, P.ep.long_row, total.p, nullptr, nullptr, P.q.p};
   out.item_counts = counts.p;
   out.count_mult = mult;
   EH_CUDA(cudaMemsetAsync(P.q.p, 0, 8, s));
@@ -1489,9 +1552,13 @@ void query_materialize(eh_context* ctx, const eh_trie* t, int query, const eh_ex
 }
 
 // One triangle / 4-clique COUNT of one trie with every piece of device
-// scratch (queue, total, views, planner arrays, scan tile sums, work items)
-// carved out of `scratch` (256-byte aligned, `bytes` long): allocates
-// nothing.  Throws EH_ERR_UNSUPPORTED when the trie needs more scratch.
+// scratch (queue, total, views, planner arrays, scan tile sums, work items,
+// and the 4-clique's per-warp S buffers when a set is too large for shared
+// memory) carved out of `scratch` (256-byte aligned, `bytes` long):
+// allocates nothing.  Throws EH_ERR_UNSUPPORTED when the trie needs more
+// scratch.  Every check that can fail before the last one is made before
+// the first launch; the last (the work plan's size) after a synchronisation,
+// so a failing call leaves no work of its own in flight.
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 void query_count_in_scratch(eh_context* ctx, const eh_trie* t, int query, const eh_exec_config* cfg,
@@ -1502,18 +1569,31 @@ void query_count_in_scratch(eh_context* ctx, const eh_trie* t, int query, const 
   EH_REQUIRE(t->ctx == ctx, EH_ERR_INVALID, "trie belongs to another context");
   ExecParams ep = exec_params(cfg);
   EH_REQUIRE(ep.shard_count == 1, EH_ERR_UNSUPPORTED, "the allocation-free path runs unsharded");
-  if (query == EH_QUERY_CLIQUE4) {
+  const bool clique = query == EH_QUERY_CLIQUE4;
+  if (clique) {
     EH_REQUIRE(t->dir != DIR_GENERAL || t->rows == 0, EH_ERR_UNSUPPORTED,
                "4-clique needs a relation that is up-, down-oriented or symmetric");
-    const int need = 2 * ((int)t->info.max_set + 1);
-    if (ep.smem_words < need) ep.smem_words = (need + 1) & ~1;
-    EH_REQUIRE((size_t)ep.smem_words * 4 * ep.warps <= 200 * 1024, EH_ERR_UNSUPPORTED,
-               "4-clique: largest set too large for the shared-memory staging");
+    size_clique_staging(ep, t->info.max_set);
   }
+  // launch shape and shared memory, checked before anything is launched
+  const int threads = 32 * ep.warps;
+  const size_t smem = (size_t)ep.smem_words * 4 * ep.warps;
+  {
+    int dev = 0, optin = 0;
+    EH_CUDA(cudaGetDevice(&dev));
+    EH_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    EH_REQUIRE(smem <= (size_t)optin, EH_ERR_UNSUPPORTED,
+               "shared staging of " + std::to_string(smem) + " bytes per block is above the device's limit of " +
+                   std::to_string(optin));
+  }
+  const void* kfn = clique ? (const void*)clique4_kernel : (const void*)triangle_kernel<MODE_COUNT>;
+  if (clique) set_smem_attr(clique4_kernel, smem);
+  else set_smem_attr(triangle_kernel<MODE_COUNT>, smem);
+  const int per_sm = blocks_per_sm(kfn, threads, smem);
   // carve the scratch
   const uint32_t nh = t->n_head;
   const uint64_t scan_elems = scan_scratch_elems(nh);
-  const size_t off_ctrl = 0;  // u32 queue, u32 error, u64 total
+  const size_t off_ctrl = 0;  // u32 queue, u32 unused, u64 total
   const size_t off_tv = 256;
   const size_t off_rv = align256(off_tv + sizeof(TrieView));
   const size_t off_nitems = align256(off_rv + sizeof(RevView));
@@ -1540,36 +1620,39 @@ void query_count_in_scratch(eh_context* ctx, const eh_trie* t, int query, const 
   EH_CUDA(cudaMemcpyAsync(dv, &hv, sizeof(TrieView), cudaMemcpyHostToDevice, s));
   EH_CUDA(cudaMemcpyAsync(dr, &hr, sizeof(RevView), cudaMemcpyHostToDevice, s));
   uint32_t n_items = 0;
+  const int pgrid = num_sms() * 4;
   if (t->rev_entries) {
-    const int pgrid = num_sms() * 4;
     plan_count_kernel<<<pgrid, 256, 0, s>>>(hr, nh, ep.chunk, nitems);
     EH_CHECK_LAUNCH();
     exclusive_scan_scratch<uint32_t>(nitems, ipos, nh, tot, scan_tmp, scan_elems, s);
     EH_CUDA(cudaMemcpyAsync(&n_items, tot, 4, cudaMemcpyDeviceToHost, s));
-    EH_CUDA(cudaStreamSynchronize(s));
-    EH_REQUIRE(off_items + sizeof(Item) * (size_t)n_items <= bytes, EH_ERR_UNSUPPORTED,
-               "trie too large for the allocation-free path: it needs " +
-                   std::to_string(off_items + sizeof(Item) * (size_t)n_items) + " bytes of scratch, the path holds " +
-                   std::to_string(bytes));
-    if (n_items) {
-      plan_fill_kernel<<<pgrid, 256, 0, s>>>(hr, nh, nitems, ipos, n_items, 0, items);
-      EH_CHECK_LAUNCH();
-    }
+  }
+  EH_CUDA(cudaStreamSynchronize(s));  // nothing of this call is in flight past here
+  const size_t items_end = align256(off_items + sizeof(Item) * (size_t)n_items);
+  EH_REQUIRE(items_end <= bytes, EH_ERR_UNSUPPORTED,
+             "trie too large for the allocation-free path: it needs " + std::to_string(items_end) +
+                 " bytes of scratch, the path holds " + std::to_string(bytes));
+  int grid = std::max(1, std::min(num_sms() * per_sm, (int)((n_items + ep.warps - 1) / ep.warps)));
+  uint32_t* gsbuf = nullptr;
+  if (clique && ep.s_cap) {
+    // one S buffer of s_cap words per resident warp, after the work items;
+    // fewer blocks when the rest of the array holds fewer buffers
+    const uint64_t per_block = (uint64_t)ep.warps * ep.s_cap * 4;
+    const uint64_t fit = (bytes - items_end) / per_block;
+    EH_REQUIRE(fit >= 1, EH_ERR_UNSUPPORTED,
+               "4-clique: the largest set (" + std::to_string(t->info.max_set) +
+                   " elements) needs S buffers of " + std::to_string(per_block) +
+                   " bytes per block, more than the allocation-free path has left");
+    grid = (int)std::min<uint64_t>((uint64_t)grid, fit);
+    gsbuf = reinterpret_cast<uint32_t*>(scratch + items_end);
   }
   if (n_items) {
-    const int threads = 32 * ep.warps;
-    const size_t smem = (size_t)ep.smem_words * 4 * ep.warps;
-    int dev = 0, optin = 0;
-    EH_CUDA(cudaGetDevice(&dev));
-    EH_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    EH_REQUIRE(smem <= (size_t)optin, EH_ERR_INVALID, "shared staging above the per-block limit");
-    const void* kfn = query == EH_QUERY_CLIQUE4 ? (const void*)clique4_kernel : (const void*)triangle_kernel<MODE_COUNT>;
-    if (query == EH_QUERY_CLIQUE4) set_smem_attr(clique4_kernel, smem);
-    else set_smem_attr(triangle_kernel<MODE_COUNT>, smem);
-    const int per_sm = blocks_per_sm(kfn, threads, smem);
-    const int grid = std::max(1, std::min(num_sms() * per_sm, (int)((n_items + ep.warps - 1) / ep.warps)));
-    QueryOut out{0, 1, ep.long_row, total, nullptr, nullptr, queue, queue + 1};
-    if (query == EH_QUERY_CLIQUE4)
+    plan_fill_kernel<<<pgrid, 256, 0, s>>>(hr, nh, nitems, ipos, n_items, 0, items);
+    EH_CHECK_LAUNCH();
+    QueryOut out{0, 1, ep.long_row, total, nullptr, nullptr, queue};
+    out.gsbuf = gsbuf;
+    out.gcap = ep.s_cap;
+    if (clique)
       clique4_kernel<<<grid, threads, smem, s>>>(dv, dr, items, n_items, ep.smem_words, out);
     else
       triangle_kernel<MODE_COUNT><<<grid, threads, smem, s>>>(dv, dr, items, n_items, ep.smem_words, out);
@@ -1579,7 +1662,7 @@ void query_count_in_scratch(eh_context* ctx, const eh_trie* t, int query, const 
   EH_CUDA(cudaMemcpyAsync(&h, total, 8, cudaMemcpyDeviceToHost, s));
   EH_CUDA(cudaStreamSynchronize(s));
   uint64_t v = h;
-  if (t->dir == DIR_SYM) v *= query == EH_QUERY_CLIQUE4 ? 24ull : 6ull;
+  if (t->dir == DIR_SYM) v *= clique ? 24ull : 6ull;
   *result = v;
 }
 
@@ -1678,7 +1761,6 @@ void batch_run(eh_context* ctx, eh_batch* b, uint64_t* results, eh_query_stats* 
     stats->work_items = b->P.n_items;
     stats->wedges = b->P.pairs;
     stats->algorithmic_bytes = 0;
-    stats->timed_out = 0;
   }
 }
 

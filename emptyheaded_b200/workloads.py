@@ -42,3 +42,16 @@ def build_chunglu_trie(E, n=1 << 23, avg_degree=32, gamma=2.1, seed=9, ctx=None,
     s.free()
     d.free()
     return t
+
+
+def golden_counts():
+    """The reference engine's counts on the seeded workloads
+    (tests/golden/golden.json, "synthetic"), for self-checking runs; {} when
+    the fixture is absent."""
+    import json
+    import os
+    p = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden", "golden.json")
+    if not os.path.exists(p):
+        return {}
+    with open(p) as f:
+        return json.load(f).get("synthetic", {})

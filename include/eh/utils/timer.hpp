@@ -1,0 +1,3 @@
+// timer.hpp -- the reference header of that name, provided by the B200 layer.
+#pragma once
+#include "../eh_dropin.hpp"

@@ -6,8 +6,9 @@
  *
  * Each entry point names the reference interface it replaces (paths are
  * relative to the EmptyHeaded repository).  The reference is a C++ template
- * library driven by generated query code; the drop-in mapping is written
- * out in INTEGRATION.md.
+ * library driven by generated query code; include/eh/ holds a C++ layer with
+ * the reference's Trie / TrieBuilder / TrieIterator / par::reducer names over
+ * this ABI, so that such code compiles and links against it.
  */
 #ifndef EH_B200_H
 #define EH_B200_H
@@ -25,7 +26,7 @@ enum {
   EH_ERR_INVALID = 1,     /* bad argument */
   EH_ERR_CUDA = 2,        /* CUDA runtime error */
   EH_ERR_OOM = 3,         /* device allocation failed */
-  EH_ERR_TIMEOUT = 4,     /* a bounded device wait gave up */
+  /* 4 is unused: no device loop here waits on another thread or device */
   EH_ERR_UNSUPPORTED = 5, /* request outside what the build supports */
   EH_ERR_IO = 6,          /* file read/write failed */
   EH_ERR_NO_DEVICE = 7    /* no CUDA device visible */
@@ -223,7 +224,6 @@ typedef struct {
                             flattened over the lanes; 0 = default (32) */
   int smem_words;        /* per-warp shared staging capacity in u32 words; 0 = default */
   int record_timings;    /* 1: log per-item device time for the cost model */
-  uint64_t spin_limit;   /* bound on device queue waits; 0 = default */
   int shard_index;       /* run work items i with i % shard_count == shard_index */
   int shard_count;       /* 0 or 1: all items (multi-GPU ranks split the plan) */
 } eh_exec_config;
@@ -235,7 +235,6 @@ typedef struct {
   uint64_t work_items;
   uint64_t wedges;       /* (v,w) pairs probed */
   uint64_t algorithmic_bytes; /* 4*sum over edges (d+(u)+d+(v)) for triangle */
-  int timed_out;
 } eh_query_stats;
 
 /* Runs one named COUNT plan over `trie` (the Edge relation in ordering
@@ -254,10 +253,16 @@ eh_status eh_query_count(eh_context* ctx, const eh_trie* trie, int query, const 
  * allocator, where a library cudaMalloc could fail and a cudaFree would
  * synchronise the device under the host's own work).  No counterpart in
  * the reference.  Runs the triangle or 4-clique plan with all its scratch
- * (work plan, queue, result) in one fixed 64 MiB device array compiled into
- * the library; calls no cudaMalloc/cudaFree.  Limit: the trie's plan must
- * fit, about 8 bytes per head entry plus 16 per work item (an R-MAT
- * scale-22 trie fits); larger tries get EH_ERR_UNSUPPORTED.  The first call
+ * (work plan, queue, result, and the 4-clique's per-warp S buffers) in one
+ * fixed 64 MiB device array compiled into the library; calls no
+ * cudaMalloc/cudaFree.  Limits: the trie's plan must fit, about 8 bytes per
+ * head entry plus 16 per work item (an R-MAT scale-22 trie fits); for the
+ * 4-clique, a largest set above what one block stages in shared memory
+ * (96 KB for the staged set and S together) needs S buffers of
+ * 4 x (largest set + 1) bytes per warp in what the plan leaves of the array
+ * (with 8 warps per block, a largest set up to about 2M elements).  Larger
+ * tries get EH_ERR_UNSUPPORTED, and the call returns with none of its GPU
+ * work in flight (at most the planner's count has run).  The first call
  * on a device looks the array up (make it before any stream capture).  Calls
  * share the array: this entry serialises its own calls per device; other
  * GPU work touching the array concurrently would race. */
@@ -344,6 +349,19 @@ eh_status eh_batch_free(eh_batch* batch);
  * lollipop/barbell, TrieBuilder::set_annotation, TrieBuilder.cpp:428-446),
  * copied to host annot[n_head]. */
 eh_status eh_triangle_annotation(eh_context* ctx, const eh_trie* trie, const eh_exec_config* cfg, uint64_t* annot);
+
+/* The root bag of the lollipop / barbell plans joined with an annotated
+ * unary relation Z(v; z) (the intermediate bag the reference materialises
+ * with TrieBuilder::set_annotation and reads back with
+ * TrieIterator::get_annotation, TrieIterator.cpp:45-59; the root bags of
+ * QueryPlannerTest.scala:199-230 as EHGenerator.scala:399-480 emits them):
+ *   EH_QUERY_LOLLIPOP: sum over head values a of z(a) * |{d : (a,d)}|
+ *   EH_QUERY_BARBELL:  sum over rows (a,x) of z(a) * z(x)
+ * z is given by value on the host: z[v] for v < n_values; values beyond
+ * and values without an annotation count 0.  Result modulo 2^64 (the
+ * reference's signed long, bit for bit). */
+eh_status eh_query_weighted_root(eh_context* ctx, const eh_trie* trie, int query, const uint64_t* z,
+                                 uint32_t n_values, uint64_t* result);
 
 /* Host-buffer convenience: copy a CSR trie (head, off, vals) from host
  * memory, lay it out with cfg, count, and return; the reference-facing

@@ -30,13 +30,18 @@ _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _lib = None
 
 
+def reference_dir():
+    """The EmptyHeaded checkout the reference engine is compiled from:
+    $EH_REFERENCE, else the directory `reference` beside this repository."""
+    return os.environ.get("EH_REFERENCE") or os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
+
+
 def build(ref=True):
     """Compile the restatement (and, when the reference tree is present, the
     reference engine driver)."""
     subprocess.check_call(["make", "-s", "-C", HERE, "restate"])
-    if ref and os.path.isdir(os.environ.get("EH_REFERENCE", "/root/reference")):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref",
-                               "REF=" + os.environ.get("EH_REFERENCE", "/root/reference")])
+    if ref and os.path.isdir(reference_dir()):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", "REF=" + reference_dir()])
 
 
 def lib():
@@ -177,6 +182,14 @@ class Trie:
 
     def barbell(self):
         return int(lib().eho_barbell(*self._args()))
+
+    def path2(self):
+        """PathAgg(;z) :- Edge(a,b),Edge(b,c) COUNT in the plan order [a,b,c]
+        (oracle/generated_bags.hpp): sum over rows (a,b) whose b heads a set
+        of |N(b)|, modulo 2^64."""
+        deg = np.zeros(int(max(self.head.max(initial=0), self.vals.max(initial=0))) + 1, np.uint64)
+        deg[self.head] = np.diff(self.off).astype(np.uint64)
+        return int(deg[self.vals].sum(dtype=np.uint64)) if len(self.vals) else 0
 
     def clique4_sel(self, v):
         """FliqueSelAgg: 4-cliques (a,b,c,d) with (a,v) in the relation."""

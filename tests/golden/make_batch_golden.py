@@ -1,7 +1,7 @@
 """Adds the 256-graph batch to golden.json: for every graph of
 emptyheaded_b200.workloads.batch256_spec() the triangle count of the
 reference engine (oracle/_ref/eh_ref) on the oracle-preprocessed rows, and
-the rows' sha1.  Needs /root/reference (built oracle); run after
+the rows' sha1.  Needs the reference checkout ($EH_REFERENCE or ../reference beside the repository; built oracle); run after
 make_golden.py."""
 import hashlib
 import json

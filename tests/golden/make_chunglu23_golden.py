@@ -3,7 +3,7 @@ Chung-Lu n = 2^23, average degree 32 (n * 16 samples), exponent 2.1,
 seed 9, symmetrised (the oracle's generator and preprocessing), counted by
 the reference engine itself (oracle/_ref/eh_ref).
 
-    python tests/golden/make_chunglu23_golden.py   (needs /root/reference and
+    python tests/golden/make_chunglu23_golden.py   (needs the reference checkout, $EH_REFERENCE or ../reference, and
                                                     oracle/_ref/eh_ref; about
                                                     10 minutes on 8 cores)"""
 import hashlib

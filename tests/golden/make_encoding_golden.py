@@ -2,7 +2,7 @@
 run through oracle/_ref/eh_ref encode) on seeded columns of each numeric
 value type it instantiates (uint32_t, int, long, float).
 
-    python tests/golden/make_encoding_golden.py   (needs /root/reference and
+    python tests/golden/make_encoding_golden.py   (needs the reference checkout, $EH_REFERENCE or ../reference, and
                                                    oracle/_ref/eh_ref)
 
 Per type: three columns sharing one encoding (the loader encodes every

@@ -1,6 +1,6 @@
 """Regenerates the golden fixtures in this directory from the reference.
 
-    python tests/golden/make_golden.py        (needs /root/reference and
+    python tests/golden/make_golden.py        (needs the reference checkout, $EH_REFERENCE or ../reference, and
                                                oracle/_ref/eh_ref, built by
                                                `make -C oracle`)
 
@@ -31,7 +31,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
 
-REF = os.environ.get("EH_REFERENCE", "/root/reference")
+REF = O.reference_dir()
 DATA = os.path.join(REF, "test", "graph", "data")
 
 
@@ -183,9 +183,11 @@ def main():
         "facebook_duplicated": {"lollipop": 1426911480, "barbell": 20371831447136},  # travis.py:29, :70
     }
     eng = {}
-    for name, a, modes in (("facebook_pruned", pruned, ("triangle", "clique4")),
-                           ("facebook_duplicated", dup, ("triangle", "lollipop", "barbell", "clique4")),
-                           ("simple", simple, ("triangle", "lollipop", "barbell", "clique4"))):
+    # path2 (Edge(a,b),Edge(b,c) COUNT) is a body no device plan runs: the
+    # C++ layer's host loop is checked on it
+    for name, a, modes in (("facebook_pruned", pruned, ("triangle", "clique4", "path2")),
+                           ("facebook_duplicated", dup, ("triangle", "lollipop", "barbell", "clique4", "path2")),
+                           ("simple", simple, ("triangle", "lollipop", "barbell", "clique4", "path2"))):
         eng[name] = {m: ref(m, a[:, 0], a[:, 1])["count_u64"] for m in modes}
     # seeded synthetic graphs, preprocessed by the oracle (bit-identical to
     # the device pipeline, checked by the GPU tests)

@@ -2,7 +2,7 @@
 (Trie::save, storage_engine/src/Trie.cpp:15-35, through oracle/_ref/eh_ref
 save), file by file, for the loader tests.
 
-    python tests/golden/make_refdb_golden.py   (needs /root/reference and
+    python tests/golden/make_refdb_golden.py   (needs the reference checkout, $EH_REFERENCE or ../reference, and
                                                 oracle/_ref/eh_ref)
 
 Entries: facebook_pruned saved with 4 threads, the oriented R-MAT-12 graph

@@ -1,6 +1,6 @@
 """Adds the equality-selection queries to golden.json.
 
-    python tests/golden/make_select_golden.py   (needs /root/reference and
+    python tests/golden/make_select_golden.py   (needs the reference checkout, $EH_REFERENCE or ../reference, and
                                                  oracle/_ref/eh_ref; run
                                                  after make_golden.py)
 

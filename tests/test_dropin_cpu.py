@@ -1,0 +1,107 @@
+"""The C++ layer of include/eh/ (the reference's Trie / TrieBuilder /
+TrieIterator / par::reducer API over the C ABI), on the CPU.
+
+The generated bag code of oracle/generated_bags.hpp -- the same source the
+reference engine runs in oracle/ref_driver.cpp -- is compiled against the
+layer and linked against a CPU test double of the C ABI
+(tests/cpp/fake_eh_abi.cpp), so the layer's symbolic pass, plan matching and
+replay run here.  Each bag must give the reference's count, and the double's
+call log shows which entry the bag went to: the device plans for the bags
+they match, the host loop over device set intersections otherwise.  A second
+build links the same program against libeh_b200.so (the product): it must
+link, and fail cleanly without a GPU."""
+import os
+import shutil
+
+import pytest
+
+from conftest import compile_dropin, run_dropin, write_facebook_tsvs
+
+pytestmark = pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+
+
+@pytest.fixture(scope="module")
+def build(tmp_path_factory):
+    d = str(tmp_path_factory.mktemp("dropin"))
+    return {"fake": compile_dropin(d, fake=True), "tsv": write_facebook_tsvs(d), "dir": d}
+
+
+def _run(build, query, graph, value=None, host_loop=False):
+    log = os.path.join(build["dir"], "calls.log")
+    if os.path.exists(log):
+        os.remove(log)
+    env = {"EH_FAKE_LOG": log}
+    if host_loop:
+        env["EH_DROPIN_HOST_LOOP"] = "1"
+    out = run_dropin(build["fake"], query, build["tsv"][graph], value, env)
+    calls = open(log).read().split() if os.path.exists(log) else []
+    return out, calls
+
+
+@pytest.mark.parametrize("query,graph,entry", [
+    ("triangle", "pruned", "eh_rule_count"),
+    ("clique4", "pruned", "eh_rule_count"),
+    ("lollipop", "duplicated", "eh_query_weighted_root:lollipop"),
+    ("barbell", "duplicated", "eh_query_weighted_root:barbell"),
+])
+def test_matching_bags_run_as_device_plans(build, golden, query, graph, entry):
+    out, calls = _run(build, query, graph)
+    assert out["count_u64"] == golden["travis"]["facebook_" + graph][query]
+    assert entry in calls
+    assert "eh_rule_count:unsupported" not in calls
+    if query in ("lollipop", "barbell"):
+        assert "eh_triangle_annotation" in calls  # the annotated bag bag_1(a;z)
+    # one intersection per outer head build (head ∩ head), none inside the loops
+    assert calls.count("eh_set_intersect_batch") <= 2
+
+
+def test_other_bodies_take_the_host_loop(build, golden):
+    """Edge(a,b),Edge(b,c) COUNT: no device plan; the generated loops run on
+    the host with each intersection on the device."""
+    out, calls = _run(build, "path2", "pruned")
+    assert out["count_u64"] == golden["reference_engine"]["facebook_pruned"]["path2"]
+    assert "eh_rule_count:unsupported" in calls
+    assert calls.count("eh_set_intersect_batch") > 1000
+
+
+def test_selection_bags(build, golden):
+    out, _ = _run(build, "barbell_sel", "duplicated", 6)
+    assert out["count_u64"] == golden["travis"]["facebook_duplicated"]["barbell_sel_p6"]
+
+
+def test_host_loop_gives_the_same_counts(build, golden):
+    out, calls = _run(build, "triangle", "pruned", host_loop=True)
+    assert out["count_u64"] == golden["travis"]["facebook_pruned"]["triangle"]
+    assert "eh_rule_count" not in calls
+    out, _ = _run(build, "lollipop", "duplicated", host_loop=True)
+    assert out["count_u64"] == golden["travis"]["facebook_duplicated"]["lollipop"]
+
+
+def test_layer_links_against_the_product_library(tmp_path):
+    """Linked against libeh_b200.so, the generated code builds; without a
+    GPU every call fails with the library's error, never a CPU answer."""
+    exe = compile_dropin(str(tmp_path), fake=False)
+    tsv = write_facebook_tsvs(str(tmp_path))["simple"]
+    out = run_dropin(exe, "triangle", tsv)
+    if "error" in out:
+        assert "device" in out["error"].lower() or "cuda" in out["error"].lower()
+
+
+def test_c_translation_unit_against_the_abi(tmp_path):
+    """A plain C99 translation unit includes include/eh_b200.h, calls the ABI
+    and links against libeh_b200.so."""
+    import subprocess
+    from conftest import LIBDIR, ROOT
+    src = tmp_path / "abi.c"
+    src.write_text('#include "eh_b200.h"\n#include <stdio.h>\n'
+                   'int main(void) { eh_context* c = 0; eh_status s = eh_context_create(0, &c);\n'
+                   '  printf("%d %s\\n", s, s ? eh_last_error() : eh_version()); if (!s) eh_context_destroy(c);\n'
+                   '  return 0; }\n')
+    exe = str(tmp_path / "abi")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I" + os.path.join(ROOT, "include"), str(src),
+                    "-L" + LIBDIR, "-leh_b200", "-Wl,-rpath," + LIBDIR, "-Wl,--allow-shlib-undefined", "-o", exe],
+                   check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0
+    status = int(r.stdout.split()[0])
+    assert status in (0, 7)  # EH_OK on a GPU box, EH_ERR_NO_DEVICE here
