@@ -201,12 +201,182 @@ def roofline(kernel_ms, alg_bytes, wedges, layout, peak, peak_kind, sm_mhz):
     return out
 
 
-def train_layout_model(E, trie, steps_per_layout=1):
-    """Profile-guided cost model: time every staged set under each layout
-    (engine-logged per-item device cycles), train the MLP on the logs with
-    the engine's own kernels, and return it with its fit statistics."""
-    from emptyheaded_b200 import learn
-    return learn.train_from_trie(E, trie, passes=steps_per_layout)
+# ------------------------------------------------------------------ timing
+def timed_counts(tr, query, cfg, steps, warmup, want, flush, step_fn=None):
+    """`warmup` untimed then `steps` timed runs of one query over a resident
+    trie (engine CUDA events: plan + kernels + count to host), the L2 flushed
+    between runs; every count is checked.  Returns (query ms list, kernel ms
+    list, launches, last stats)."""
+    import torch
+    run = step_fn or (lambda: tr.count(query, stats=True, config=cfg))
+    for _ in range(warmup):
+        c, _ = run()
+        assert c == want, (query, c, want)
+    torch.cuda.synchronize()
+    qms, kms, launches, st = [], [], 0, None
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        c, st = run()
+        assert c == want, (query, c, want)
+        qms.append(st["query_ms"])
+        kms.append(st["kernel_ms"])
+        launches += st["launches"]
+    return qms, kms, launches, st
+
+
+def _ms(x):
+    return {"mean_ms": statistics.mean(x), "median_ms": statistics.median(x)}
+
+
+# --------------------------------------------------- the other workloads
+def other_workloads(E, ctx, args, flush, deadline, model22):
+    """North-star configs beside the headline: the 256-graph batch, the
+    R-MAT-20 4-clique, Chung-Lu 2^23 lollipop and barbell; each with the
+    density-rule and learned layouts on the device (identical counts) and the
+    reference engine on this host's cores (in the same run) on a stated
+    sample.  Skipped once `deadline` (time.time()) has passed."""
+    import numpy as np
+    from emptyheaded_b200 import autotune as AT, learn, workloads as W
+    from oracle import oracle as O
+    gold = W.golden_counts()
+    out = {}
+    ref_ok = O.ref_available()
+    steps = max(3, min(args.steps, 5))
+
+    def over():
+        return time.time() > deadline
+
+    # ---- 256 R-MAT graphs (scales 10..18), triangle COUNT, one CUDA-graph replay
+    if not over():
+        try:
+            spec = W.batch256_spec()
+            want = [int(x["triangle"]) for x in json.load(open(os.path.join(ROOT, "tests", "golden", "golden.json")))
+                    ["batch256"]]
+            tries = [W.build_rmat_trie(E, sc, sd, ctx=ctx) for sc, sd in spec]
+
+            def run_batch(tag):
+                b = E.Batch(tries)
+                res = b.run()
+                assert [int(x) for x in res] == want, tag
+                ms = []
+                for _ in range(steps):
+                    flush.zero_()
+                    torch_sync()
+                    r, st = b.run(stats=True)
+                    assert [int(x) for x in r] == want, tag
+                    ms.append(st["query_ms"])
+                b.free()
+                return ms
+
+            ms_h = run_batch("heuristic")
+            for t in tries:  # the R-MAT-22 triangle model, never trained on these graphs
+                t.relayout(policy=E.LEARNED, model=model22)
+            ms_l = run_batch("learned")
+            rows = int(sum(t.info()["rows"] for t in tries))
+            for t in tries:
+                t.free()
+            rec = {"graphs": len(spec), "rows": rows, "launches_per_run": 1, "heuristic": _ms(ms_h),
+                   "learned": _ms(ms_l), "learned_speedup": statistics.mean(ms_h) / statistics.mean(ms_l),
+                   "model": "trained on R-MAT-22 triangle logs (held out: none of these graphs)"}
+            if ref_ok and not args.no_cpu:
+                # the reference engine graph by graph until ~20 s of its query time; scaled to all rows
+                t0, q, done_rows, done = time.time(), 0.0, 0, 0
+                order = list(range(len(spec)))
+                for i in order:
+                    sc, sd = spec[i]
+                    u, v = O.gen_rmat(sd, sc, 16 << sc, *ABCD)
+                    s_, d_, _ = O.preprocess(u, v)
+                    r = O.ref_query_edges("triangle", s_, d_, repeats=1, timeout=300)
+                    assert r["count_u64"] == want[i]
+                    q += r["query_s"][0]
+                    done_rows += len(s_)
+                    done += 1
+                    if time.time() - t0 > 25 or over():
+                        break
+                rec["cpu_baseline"] = {"value": 1e3 * q * rows / max(1, done_rows), "unit": "ms",
+                                       "cores": r["threads"], "kind": "reference",
+                                       "sample": "%d of %d graphs (%d of %d rows), query time summed and scaled "
+                                                 "by rows" % (done, len(spec), done_rows, rows)}
+            out["batch256_triangle"] = rec
+        except Exception as ex:
+            out["batch256_triangle"] = {"error": repr(ex)[:300]}
+
+    # ---- R-MAT-20 4-clique: a cost model trained on the 4-clique kernel's own logs
+    if not over():
+        try:
+            want = int(gold["rmat_s20_ef16_s42"]["clique4"])
+            t = W.build_rmat_trie(E, 20, SEED, ctx=ctx)
+            cfg = dict(AT.DEFAULT)
+            qh, kh, _, _ = timed_counts(t, "clique4", cfg, steps, 2, want, flush)
+            m4, info4, prof4 = learn.train_from_trie(E, t, passes=1, epochs=40, query="clique4")
+            t.relayout(policy=E.LEARNED, model=m4)
+            ql, kl, _, _ = timed_counts(t, "clique4", cfg, steps, 2, want, flush)
+            t.relayout(policy=E.EXPLICIT, layouts=learn.best_layouts(prof4))
+            qb, _, _, _ = timed_counts(t, "clique4", cfg, steps, 2, want, flush)
+            rec = {"rows": t.info()["rows"], "count": want, "heuristic": _ms(qh), "learned": _ms(ql),
+                   "exhaustive_best": _ms(qb), "learned_speedup": statistics.mean(qh) / statistics.mean(ql),
+                   "model": {k: info4[k] for k in ("median_abs_pct_error", "regret_learned_pct",
+                                                  "regret_heuristic_pct", "sets_staged") if k in info4}}
+            t.free()
+            m4.free()
+            if ref_ok and not args.no_cpu and not over():
+                u, v = O.gen_rmat(SEED, 20, 16 << 20, *ABCD)
+                s_, d_, _ = O.preprocess(u, v)
+                r = O.ref_query_edges("clique4", s_, d_, repeats=1, timeout=600)
+                assert r["count_u64"] == want
+                rec["cpu_baseline"] = {"value": 1e3 * r["query_s"][0], "unit": "ms", "cores": r["threads"],
+                                       "kind": "reference", "sample": "full R-MAT-20 4-clique COUNT, one run, "
+                                                                      "trie build excluded"}
+            out["rmat20_clique4"] = rec
+        except Exception as ex:
+            out["rmat20_clique4"] = {"error": repr(ex)[:300]}
+
+    # ---- Chung-Lu 2^23 lollipop / barbell: a model trained on the annotated pass's logs
+    if not over():
+        try:
+            g23 = gold["chunglu_n8388608_d32_g2.1_s9_sym"]
+            t = W.build_chunglu_trie(E, ctx=ctx)
+            cfg = dict(AT.DEFAULT)
+            rec = {"rows": t.info()["rows"]}
+            res = {}
+            for q in ("lollipop", "barbell"):
+                res[q] = timed_counts(t, q, cfg, 3, 1, int(g23[q]), flush)[0]
+            mc, infoc, _ = learn.train_from_trie(E, t, passes=1, epochs=40, query="lollipop")
+            t.relayout(policy=E.LEARNED, model=mc)
+            for q in ("lollipop", "barbell"):
+                ql = timed_counts(t, q, cfg, 3, 1, int(g23[q]), flush)[0]
+                rec[q] = {"count": int(g23[q]), "heuristic": _ms(res[q]), "learned": _ms(ql),
+                          "learned_speedup": statistics.mean(res[q]) / statistics.mean(ql)}
+            rec["model"] = {k: infoc[k] for k in ("median_abs_pct_error", "regret_learned_pct",
+                                                  "regret_heuristic_pct", "sets_staged") if k in infoc}
+            t.free()
+            mc.free()
+            if ref_ok and not args.no_cpu and not over():
+                # the reference engine on a bounded sample: the same generator at n = 2^19
+                # (its queries at 2^23 take minutes); the device on the same sample beside it
+                n = 1 << 19
+                u, v = O.gen_chunglu(9, n, n * 16, 2.1)
+                s_, d_, _ = O.preprocess(u, v, symmetric=True)
+                ts = E.Trie(s_, d_, ctx=ctx)
+                for q in ("lollipop", "barbell"):
+                    r = O.ref_query_edges(q, s_, d_, repeats=1, timeout=600)
+                    dev = timed_counts(ts, q, cfg, 3, 1, r["count_u64"], flush)[0]
+                    rec[q]["cpu_baseline"] = {"value": 1e3 * r["query_s"][0], "unit": "ms", "cores": r["threads"],
+                                              "kind": "reference",
+                                              "sample": "Chung-Lu n=2^19 (same generator, average degree 32, "
+                                                        "exponent 2.1), one run; device on the same sample: "
+                                                        "%.2f ms (density rule)" % statistics.mean(dev)}
+                ts.free()
+            out["chunglu23_lollipop_barbell"] = rec
+        except Exception as ex:
+            out["chunglu23_lollipop_barbell"] = {"error": repr(ex)[:300]}
+    return out
+
+
+def torch_sync():
+    import torch
+    torch.cuda.synchronize()
 
 
 def ours_arm(args):
@@ -219,10 +389,13 @@ def ours_arm(args):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
     import emptyheaded_b200 as E
+    from emptyheaded_b200 import autotune as AT, learn, shard as SH, workloads as W
 
+    t_start = time.time()
     ctx = E.Context(local if world > 1 else 0)
     E._default = ctx
     g = golden()
+    want = g["triangle"]
     # ---- input pipeline and trie build (untimed, like the reference's load)
     t0 = time.time()
     u, v = E.gen_rmat(SEED, SCALE, EF << SCALE, *ABCD, ctx=ctx)
@@ -232,76 +405,50 @@ def ours_arm(args):
     trie = E.Trie(s, d, ctx=ctx)
     info_h = trie.info()
     build_s = time.time() - t0
-
     shard = (rank, world)
+    flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")  # 256 MB > L2
 
-    from emptyheaded_b200 import shard as SH
-
-    from emptyheaded_b200 import autotune as AT
-
-    def step(tr, cfg):
-        c, st = tr.count("triangle", stats=True, shard=shard, config=cfg)
+    def step(cfg):
+        c, st = trie.count("triangle", stats=True, shard=shard, config=cfg)
         if world > 1:
             c = SH.combine_counts(c, device="cuda")
         return c, st
 
-    def tune(tr):
-        # every rank must cut the same plan (the chunk size sets the items),
-        # so only a single-GPU run tunes
-        if world > 1:
-            return dict(AT.DEFAULT), []
-        return AT.tune(tr)
+    def tune():
+        # every rank must cut the same plan (the chunk size sets the items)
+        return dict(AT.DEFAULT) if world > 1 else AT.tune(trie)[0]
 
-    # L2 flush buffer (larger than the 126 MB L2)
-    flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")
-
-    def timed(tr, steps, warmup, cfg):
-        for _ in range(warmup):
-            c, _ = step(tr, cfg)
-            assert c == g["triangle"], c
+    def timed(cfg):
         if world > 1:
             torch.distributed.barrier()
-        torch.cuda.synchronize()
-        qms, kms, launches = [], [], 0
-        wall0 = time.time()
-        # NVTX range "timed": profiler captures select the timed steps with
-        # --nvtx --nvtx-include "timed/"
-        torch.cuda.nvtx.range_push("timed")
-        for _ in range(steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            c, st = step(tr, cfg)
-            assert c == g["triangle"], c
-            qms.append(st["query_ms"])
-            kms.append(st["kernel_ms"])
-            launches += st["launches"]
-        torch.cuda.synchronize()
-        torch.cuda.nvtx.range_pop()
+        r = timed_counts(trie, "triangle", cfg, args.steps, args.warmup, want, flush, lambda: step(cfg))
         if world > 1:
             torch.distributed.barrier()
-        wall = time.time() - wall0
-        return qms, kms, launches, st, wall
+        return r
 
-    # ---- heuristic layouts (schedule autotuned for them, untimed)
-    cfg_h, tlog_h = tune(trie)
+    def rmax(x):
+        return x if world == 1 else SH.max_over_ranks(x, device="cuda")
+
+    # ---- density-rule layouts (schedule autotuned for them, untimed)
+    cfg_h = tune()
     # clocks are sampled over the device-timed steps only: nvidia-smi's driver
     # queries stall host-side CUDA calls, which the e2e leg measures
     args.sampler.start()
-    qh, kh, lh, st_h, wall_h = timed(trie, args.steps, args.warmup, cfg_h)
-    # ---- learned layouts (model trained on this engine's logged timings)
-    learn_info = {}
-    cfg_l = cfg_h
+    qh, kh, lh, st_h = timed(cfg_h)
+    # ---- learned layouts: the cost model trained on this engine's logged timings
+    learn_info, extra_layouts = {}, {}
+    model = None
+    cfg_l, ql, kl, ll, st_l = cfg_h, qh, kh, lh, st_h
     try:
         if world > 1:
             # every rank must cut the same plan from the same layouts and
             # predicted costs: rank 0 trains the model, the others load its
             # parameters (the same collectives on every rank, failure included)
-            from emptyheaded_b200 import learn as LN
             ok = torch.zeros(1, device="cuda")
-            model = E.Model(LN.DIMS, ctx=ctx)
+            model = E.Model(learn.DIMS, ctx=ctx)
             if rank == 0:
                 try:
-                    model, learn_info = train_layout_model(E, trie)
+                    model, learn_info, _ = learn.train_from_trie(E, trie, passes=1)
                     ok.fill_(1)
                 except Exception as ex:
                     learn_info = {"error": repr(ex)[:300]}
@@ -312,27 +459,41 @@ def ours_arm(args):
             torch.distributed.broadcast(p, 0)
             model.set_params(p.cpu().numpy())
         else:
-            model, learn_info = train_layout_model(E, trie)
+            prof = learn.profile(E, trie, reps=2)
+            model, learn_info, _ = learn.train_from_trie(E, trie, prof=prof)
+            learn_info["evaluated_on"] = "the R-MAT-22 profile it was trained on (in sample)"
+            # a model trained on another graph (R-MAT-20), judged on this one
+            t20 = W.build_rmat_trie(E, 20, SEED, ctx=ctx)
+            model_ho, info20, _ = learn.train_from_trie(E, t20, passes=2)
+            t20.free()
+            ho = learn.evaluate(E, model_ho, prof)
+            ho["trained_on"] = "R-MAT-20 seed 42 triangle logs; evaluated on the R-MAT-22 profile (held out)"
+            trie.relayout(policy=E.LEARNED, model=model_ho)
+            cfg_ho = tune()
+            qo, ko, _, _ = timed(cfg_ho)
+            ho.update({"query": _ms(qo), "kernel": _ms(ko), "speedup_vs_heuristic": statistics.mean(qh) /
+                       statistics.mean(qo), "layout_hist": _hist(trie.info())})
+            extra_layouts["learned_held_out"] = ho
+            # the per-set exhaustive search's own assignment: the ceiling of any layout policy
+            trie.relayout(policy=E.EXPLICIT, layouts=learn.best_layouts(prof))
+            cfg_b = tune()
+            qb, kb, _, _ = timed(cfg_b)
+            extra_layouts["exhaustive_best"] = {"query": _ms(qb), "kernel": _ms(kb), "schedule": cfg_b,
+                                                "speedup_vs_heuristic": statistics.mean(qh) / statistics.mean(qb),
+                                                "layout_hist": _hist(trie.info())}
+            model_ho.free()
         trie.relayout(policy=E.LEARNED, model=model)
-        info_l = trie.info()
-        cfg_l, tlog_l = tune(trie)
-        ql, kl, ll, st_l, wall_l = timed(trie, args.steps, args.warmup, cfg_l)
-        learn_info["layout_hist"] = {"uint": info_l["n_uinteger"], "bitset": info_l["n_range_bitset"],
-                                     "block": info_l["n_block_bitset"]}
+        learn_info["layout_hist"] = _hist(trie.info())
+        cfg_l = tune()
+        ql, kl, ll, st_l = timed(cfg_l)
     except Exception as ex:  # the learned arm must not hide the measurement
         learn_info = {"error": repr(ex)[:300]}
-        ql, kl, ll, st_l, wall_l = qh, kh, lh, st_h, wall_h
+        model = None
     clocks = args.sampler.stop()
 
-    def rmax(x):
-        return x if world == 1 else SH.max_over_ranks(x, device="cuda")
-
-    ms_h = rmax(statistics.mean(qh))
-    ms_l = rmax(statistics.mean(ql))
-    kern_l = rmax(statistics.mean(kl))
-    kern_h = rmax(statistics.mean(kh))
-    med_h = rmax(statistics.median(qh))
-    med_l = rmax(statistics.median(ql))
+    ms_h, ms_l = rmax(statistics.mean(qh)), rmax(statistics.mean(ql))
+    kern_h, kern_l = rmax(statistics.mean(kh)), rmax(statistics.mean(kl))
+    med_h, med_l = rmax(statistics.median(qh)), rmax(statistics.median(ql))
 
     # ---- e2e through the host-buffer entry: CSR in pinned host memory,
     # copied to the device every step (plus the trie index build), count back
@@ -343,26 +504,25 @@ def ours_arm(args):
         off_p = torch.from_numpy(off.view(np.int64)).pin_memory().numpy().view(np.uint64)
         vals_p = torch.from_numpy(vals.view(np.int32)).pin_memory().numpy().view(np.uint32)
         h2d = head_p.nbytes + off_p.nbytes + vals_p.nbytes
-        pol = E.LEARNED if "error" not in learn_info else E.HEURISTIC
-        mdl = model if "error" not in learn_info else None
+        pol = E.LEARNED if model is not None else E.HEURISTIC
         # one call measures its peak device memory; the pool then keeps that
         # much (plus slack) as one block, so no timed call maps new memory
         used0 = ctx.memory()["used"]
         ctx.reserve(0)
-        c = E.count_host_csr(head_p, off_p, vals_p, nodes, policy=pol, model=mdl, ctx=ctx, config=cfg_l)
-        assert c == g["triangle"]
+        c = E.count_host_csr(head_p, off_p, vals_p, nodes, policy=pol, model=model, ctx=ctx, config=cfg_l)
+        assert c == want
         pool_bytes = int(1.1 * (ctx.memory()["peak"] - used0)) + (64 << 20)
         ctx.reserve(pool_bytes)
         for _ in range(max(3, args.warmup)):
-            c = E.count_host_csr(head_p, off_p, vals_p, nodes, policy=pol, model=mdl, ctx=ctx, config=cfg_l)
-            assert c == g["triangle"]
+            c = E.count_host_csr(head_p, off_p, vals_p, nodes, policy=pol, model=model, ctx=ctx, config=cfg_l)
+            assert c == want
         ev = []
         for _ in range(max(3, args.steps)):
             torch.cuda.synchronize()
             a = time.perf_counter()
-            c = E.count_host_csr(head_p, off_p, vals_p, nodes, policy=pol, model=mdl, ctx=ctx, config=cfg_l)
+            c = E.count_host_csr(head_p, off_p, vals_p, nodes, policy=pol, model=model, ctx=ctx, config=cfg_l)
             ev.append(1e3 * (time.perf_counter() - a))
-            assert c == g["triangle"]
+            assert c == want
         e2e = {"value": statistics.median(ev), "unit": "ms", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8,
                "path": "eh_query_count_host_csr: pinned host CSR -> device, trie index + layouts, count, result to host",
                "runs_ms": [round(x, 2) for x in ev], "pool_reserved_bytes": pool_bytes}
@@ -379,20 +539,28 @@ def ours_arm(args):
                        "sample": "full R-MAT-22 triangle COUNT, median of 3 runs, trie build excluded "
                                  "(reference build %.1f s, sort serialised)" % r["build_s"],
                        "count": r["count_u64"]}
-                assert r["count_u64"] == g["triangle"]
+                assert r["count_u64"] == want
         except Exception as ex:
             cpu = {"value": None, "unit": "ms", "cores": cpu_threads(), "kind": "reference", "sample": repr(ex)[:200]}
+    s.free()
+    d.free()
+    trie.free()
+
+    # ---- the north-star configs beside the headline (single GPU)
+    workloads = None
+    if world == 1 and not args.no_extra and model is not None:
+        workloads = other_workloads(E, ctx, args, flush, t_start + args.budget_s, model)
 
     if rank == 0:
         peak, peak_kind = load_peaks()
-        layout_name = "learned" if "error" not in learn_info else "heuristic"
+        layout_name = "learned" if model is not None else "heuristic"
         roof = roofline(kern_l, st_l["algorithmic_bytes"], st_l["wedges"], layout_name, peak,
                         peak_kind + " (hbm_gbs)", clocks.get("sm_mhz"))
         line = {
             "metric": METRIC, "value": ms_l, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_l, "higher_is_better": False, "scaling": "strong",
             "vs_baseline": None, "dtype": "uint32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "rows": info_h["rows"], "nodes": nodes, "layout": "learned",
+            "config": {"workload": WORKLOAD, "rows": info_h["rows"], "nodes": nodes, "layout": layout_name,
                        "heuristic_ms": ms_h, "learned_ms": ms_l, "learned_speedup": ms_h / ms_l,
                        "heuristic_kernel_ms": kern_h, "learned_kernel_ms": kern_l,
                        "heuristic_median_ms": med_h, "learned_median_ms": med_l,
@@ -400,19 +568,24 @@ def ours_arm(args):
                              % (info_h["device_bytes"] / 1e9),
                        "trie_build_s": build_s, "parallelism": "shards of work items" if world > 1 else "single GPU",
                        "schedule_heuristic": cfg_h, "schedule_learned": cfg_l,
-                       "learned": learn_info},
-            "count": g["triangle"],
+                       "learned": learn_info, "layouts_compared": extra_layouts},
+            "count": want,
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(ll / max(1, args.steps)) * args.steps,
+            "workloads": workloads,
         }
         line["clocks"] = clocks
         print(json.dumps(line), flush=True)
-    trie.free()
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def _hist(info):
+    return {"uint": info["n_uinteger"], "bitset": info["n_range_bitset"], "block": info["n_block_bitset"],
+            "bitset_words": info["bitset_words"], "device_bytes": info["device_bytes"]}
 
 
 def case_arm(args):
@@ -430,21 +603,23 @@ def case_arm(args):
     forced = {"uint": E.UINTEGER, "bitset": E.RANGE_BITSET, "block": E.BLOCK_BITSET}
     learn_info = None
     if args.layout == "learned":
-        model, learn_info = learn.train_from_trie(E, t)
+        model, learn_info, _ = learn.train_from_trie(E, t)
         t.relayout(policy=E.LEARNED, model=model)
     elif args.layout in forced:
         t.relayout(policy=E.FORCED, forced=forced[args.layout], max_bitset_bytes=1 << 50)
     runs = []
-    t.count(args.query)  # warm
+    bi = not args.no_block_items
+    t.count(args.query, block_items=bi)  # warm
     torch.cuda.nvtx.range_push("case")
     for _ in range(args.repeat):
-        c, st = t.count(args.query, stats=True)
+        c, st = t.count(args.query, stats=True, block_items=bi)
         runs.append({"count": c, "query_ms": st["query_ms"], "kernel_ms": st["kernel_ms"], "wedges": st["wedges"],
                      "algorithmic_bytes": st["algorithmic_bytes"]})
     torch.cuda.nvtx.range_pop()
     g = W.golden_counts().get("rmat_s%d_ef16_s%d" % (args.scale, SEED), {})
     ok = all(r["count"] == g[args.query] for r in runs) if args.query in g else None
     print(json.dumps({"case": "rmat%d" % args.scale, "query": args.query, "layout": args.layout, "ok": ok,
+                      "block_items": bi,
                       "info": t.info(), "learned": learn_info, "runs": runs}))
     t.free()
     return 0 if ok in (None, True) else 1
@@ -456,13 +631,17 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline legs")
+    ap.add_argument("--no-extra", action="store_true", help="headline only: skip the other north-star configs")
+    ap.add_argument("--budget-s", type=float, default=300.0,
+                    help="wall-clock budget after which the remaining other configs are skipped")
     ap.add_argument("--case", action="store_true", help="profiler case instead of the bench line")
     ap.add_argument("--scale", type=int, default=20, help="--case: R-MAT scale")
     ap.add_argument("--layout", default="heuristic", choices=["heuristic", "learned", "uint", "bitset", "block"],
                     help="--case: layout policy")
     ap.add_argument("--query", default="triangle", help="--case: query")
     ap.add_argument("--repeat", type=int, default=2, help="--case: runs inside the NVTX range")
+    ap.add_argument("--no-block-items", action="store_true", help="--case: stage every N(b) per warp")
     args = ap.parse_args()
     if args.case:
         return case_arm(args)

@@ -31,7 +31,7 @@ LIB_PATH = os.environ.get("EH_B200_LIB") or os.path.join(_HERE, "_lib", "libeh_b
 EH_OK = 0
 STATUS_NAMES = {1: "INVALID", 2: "CUDA", 3: "OOM", 5: "UNSUPPORTED", 6: "IO", 7: "NO_DEVICE"}
 RANGE_BITSET, UINTEGER, BLOCK_BITSET = 0, 1, 3
-HEURISTIC, LEARNED, FORCED = 0, 1, 2
+HEURISTIC, LEARNED, FORCED, EXPLICIT = 0, 1, 2, 3
 QUERIES = {"triangle": 0, "clique4": 1, "lollipop": 2, "barbell": 3}
 # equality-selection plans (Trie.count_select)
 SELECT_QUERIES = {"clique4_sel": 4, "barbell_sel": 5}
@@ -46,7 +46,7 @@ class EHError(RuntimeError):
 
 class LayoutConfig(ctypes.Structure):
     _fields_ = [("policy", ctypes.c_int), ("forced_layout", ctypes.c_int), ("model", ctypes.c_void_p),
-                ("max_bitset_bytes", ctypes.c_uint64)]
+                ("max_bitset_bytes", ctypes.c_uint64), ("layouts", ctypes.c_void_p)]
 
 
 class TrieInfo(ctypes.Structure):
@@ -60,7 +60,7 @@ class TrieInfo(ctypes.Structure):
 class ExecConfig(ctypes.Structure):
     _fields_ = [("warps_per_block", ctypes.c_int), ("chunk_pairs", ctypes.c_int), ("long_row", ctypes.c_int),
                 ("smem_words", ctypes.c_int), ("record_timings", ctypes.c_int),
-                ("shard_index", ctypes.c_int), ("shard_count", ctypes.c_int)]
+                ("shard_index", ctypes.c_int), ("shard_count", ctypes.c_int), ("no_block_items", ctypes.c_int)]
 
 
 class Atom(ctypes.Structure):
@@ -305,17 +305,22 @@ def preprocess(u, v, symmetric=False, ctx=None):
     return DeviceArray(ctx, s.value, rows.value), DeviceArray(ctx, d.value, rows.value), nodes.value
 
 
-def _layout_cfg(policy=HEURISTIC, forced=UINTEGER, model=None, max_bitset_bytes=0):
+def _layout_cfg(policy=HEURISTIC, forced=UINTEGER, model=None, max_bitset_bytes=0, layouts=None):
     c = LayoutConfig()
     c.policy = policy
     c.forced_layout = forced
     c.model = model.h.value if model is not None else None
     c.max_bitset_bytes = max_bitset_bytes
+    c._keep = None
+    if layouts is not None:
+        c._keep = np.ascontiguousarray(layouts, np.uint8)
+        c.layouts = c._keep.ctypes.data
     return c
 
 
-def _exec_cfg(warps=0, chunk=0, smem_words=0, record=False, shard=(0, 1), long_row=0):
+def _exec_cfg(warps=0, chunk=0, smem_words=0, record=False, shard=(0, 1), long_row=0, block_items=True):
     e = ExecConfig()
+    e.no_block_items = 0 if block_items else 1
     e.warps_per_block = warps
     e.chunk_pairs = chunk
     e.long_row = long_row
@@ -386,8 +391,10 @@ class Trie:
         _check(lib().eh_trie_info_get(self.h, ctypes.byref(i)))
         return {k: getattr(i, k) for k, _ in TrieInfo._fields_}
 
-    def relayout(self, policy=HEURISTIC, forced=UINTEGER, model=None, max_bitset_bytes=0):
-        cfg = _layout_cfg(policy, forced, model, max_bitset_bytes)
+    def relayout(self, policy=HEURISTIC, forced=UINTEGER, model=None, max_bitset_bytes=0, layouts=None):
+        """Re-pick the level-1 layouts: the density rule, the learned model,
+        one forced layout, or (policy=EXPLICIT) one layout per set."""
+        cfg = _layout_cfg(policy, forced, model, max_bitset_bytes, layouts)
         _check(lib().eh_trie_relayout(self.ctx.h, self.h, ctypes.byref(cfg)))
 
     def export(self):
@@ -412,7 +419,7 @@ class Trie:
         return out[: n.value], lay.value
 
     def count(self, query="triangle", warps=0, chunk=0, smem_words=0, record=False, stats=False, shard=(0, 1),
-              long_row=0, config=None):
+              long_row=0, config=None, block_items=True):
         """Run a named COUNT plan; returns the count (and stats if asked).
         shard=(i, n) runs the i-th of n round-robin shares of the work items
         (the partial counts of the n shares sum to the count).  `config`
@@ -422,7 +429,8 @@ class Trie:
             chunk = config.get("chunk", chunk)
             smem_words = config.get("smem_words", smem_words)
             long_row = config.get("long_row", long_row)
-        e = _exec_cfg(warps, chunk, smem_words, record, shard, long_row)
+            block_items = config.get("block_items", block_items)
+        e = _exec_cfg(warps, chunk, smem_words, record, shard, long_row, block_items)
         r = ctypes.c_uint64()
         st = QueryStats()
         _check(lib().eh_query_count(self.ctx.h, self.h, QUERIES[query], ctypes.byref(e), ctypes.byref(r),

@@ -195,6 +195,7 @@ template <typename T>
 void exclusive_scan(const T* in, T* out, uint64_t n, T* total_dev, cudaStream_t s);
 // The same with its tile sums in caller memory; allocates nothing.
 uint64_t scan_scratch_elems(uint64_t n);
+uint32_t scan_launches(uint64_t n);
 template <typename T>
 void exclusive_scan_scratch(const T* in, T* out, uint64_t n, T* total_dev, T* scratch, uint64_t scratch_elems,
                             cudaStream_t s);

@@ -97,6 +97,13 @@ void exclusive_scan(const T* in, T* out, uint64_t n, T* total_dev, cudaStream_t 
 template void exclusive_scan<uint32_t>(const uint32_t*, uint32_t*, uint64_t, uint32_t*, cudaStream_t);
 template void exclusive_scan<uint64_t>(const uint64_t*, uint64_t*, uint64_t, uint64_t*, cudaStream_t);
 
+// Kernels exclusive_scan launches for n inputs.
+uint32_t scan_launches(uint64_t n) {
+  if (n == 0) return 0;
+  const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+  return tiles == 1 ? 1u : 2u + scan_launches(tiles);
+}
+
 // Tile-sum elements exclusive_scan_scratch needs for n inputs (all levels).
 uint64_t scan_scratch_elems(uint64_t n) {
   uint64_t need = 0;

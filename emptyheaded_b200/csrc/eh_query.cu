@@ -73,6 +73,7 @@ struct ExecParams {
   uint32_t long_row;
   uint32_t s_cap;  // 4-clique: S buffers in global memory of this many words per warp (0: in shared memory)
   bool smem_given; // the caller chose smem_words
+  bool no_block_items;  // stage every N(b) per warp (no block items)
 };
 
 static ExecParams exec_params(const eh_exec_config* cfg) {
@@ -86,6 +87,7 @@ static ExecParams exec_params(const eh_exec_config* cfg) {
   EH_REQUIRE(p.shard_index < p.shard_count, EH_ERR_INVALID, "shard_index must be below shard_count");
   p.s_cap = 0;
   p.smem_given = cfg && cfg->smem_words > 0;
+  p.no_block_items = cfg && cfg->no_block_items;
   p.warps = std::max(1, std::min(p.warps, kMaxWarps));
   p.smem_words = std::max(64, std::min(p.smem_words, 16384)) & ~1;
   return p;
@@ -97,20 +99,6 @@ __global__ void plan_count_kernel(RevView r, uint32_t nh, uint32_t chunk, uint32
   for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nh; b += gridDim.x * blockDim.x) {
     const uint64_t w = r.rev_wpre[r.rev_off[b + 1]] - r.rev_wpre[r.rev_off[b]];
     nitems[b] = (uint32_t)((w + chunk - 1) / chunk);
-  }
-}
-// the same from the cost model's predicted cycles of b's work (learned
-// layouts): items of about `unit` predicted cycles, at most one per 64 probes
-__global__ void plan_count_pred_kernel(RevView r, uint32_t nh, const float* __restrict__ pred, double unit,
-                                       uint32_t* __restrict__ nitems) {
-  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nh; b += gridDim.x * blockDim.x) {
-    const uint64_t w = r.rev_wpre[r.rev_off[b + 1]] - r.rev_wpre[r.rev_off[b]];
-    uint64_t n = 0;
-    if (w) {
-      n = (uint64_t)ceil((double)pred[b] / unit);
-      n = max((uint64_t)1, min(n, (w + 63) / 64));
-    }
-    nitems[b] = (uint32_t)n;
   }
 }
 // item i of b covers the rows whose work prefix falls in [i, i+1) * W/n;
@@ -143,33 +131,84 @@ __global__ void plan_fill_kernel(RevView r, uint32_t nh, const uint32_t* __restr
   }
 }
 
-struct Plan {
-  DevBuf<Item> items;
-  uint32_t n = 0;
+// Work of head entry b is staged in one of two classes: per warp (N(b)
+// fits a warp's shared region, or must be probed in global memory) or per
+// block (N(b) needs more than a warp's region but fits the block's: every
+// warp of the block works on the rows of one staged N(b)).  A block item
+// holds `warps` times a warp item's work.
+__device__ __forceinline__ uint32_t staged_words(const TrieView& t, uint32_t b) {
+  const uint8_t l = t.layout[b];
+  if (l == EH_LAYOUT_RANGE_BITSET) return 2u * t.aux[b].n;
+  if (l == EH_LAYOUT_UINTEGER) return (uint32_t)(t.off[b + 1] - t.off[b]);
+  return 0xffffffffu;  // block bitsets are probed in global memory
+}
+
+struct PlanShape {
+  uint32_t chunk;        // probes per warp item
+  const float* pred;     // predicted cycles of each head entry's work (learned layouts), or null
+  double unit;           // predicted cycles per warp item
+  uint32_t warp_words;   // staging capacity of a warp (u32 words)
+  uint32_t block_words;  // staging capacity of a block; 0: no block items
+  uint32_t warps;        // warps per block
 };
 
-static void build_plan(eh_context* ctx, const eh_trie* t, uint32_t chunk, uint32_t g, Plan& plan) {
+__global__ void plan_split_kernel(TrieView t, RevView r, PlanShape ps, uint32_t* __restrict__ nw,
+                                  uint32_t* __restrict__ nb) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.n_head; b += gridDim.x * blockDim.x) {
+    const uint64_t w = r.rev_wpre[r.rev_off[b + 1]] - r.rev_wpre[r.rev_off[b]];
+    const uint32_t sw = staged_words(t, b);
+    const bool blk = ps.block_words && sw > ps.warp_words && sw <= ps.block_words;
+    const uint64_t mult = blk ? ps.warps : 1;
+    uint64_t n = 0;
+    if (w) {
+      if (ps.pred) {
+        n = (uint64_t)ceil((double)ps.pred[b] / (ps.unit * (double)mult));
+        n = max((uint64_t)1, min(n, (w + 63) / 64));
+      } else {
+        n = (w + ps.chunk * mult - 1) / (ps.chunk * mult);
+      }
+    }
+    nw[b] = blk ? 0u : (uint32_t)n;
+    nb[b] = blk ? (uint32_t)n : 0u;
+  }
+}
+
+struct Plan {
+  DevBuf<Item> items;  // block items first, then warp items
+  uint32_t n = 0;      // all items
+  uint32_t nb = 0;     // block items
+};
+
+// returns the kernels it launched
+static uint32_t build_plan(eh_context* ctx, const eh_trie* t, const PlanShape& shape, uint32_t g, Plan& plan) {
   cudaStream_t s = ctx->stream;
-  plan.n = 0;
-  if (!t->rev_entries) return;
+  plan.n = plan.nb = 0;
+  if (!t->rev_entries) return 0;
   RevView r{t->rev_off.p, t->rev_lo.p, t->rev_hi.p, t->rev_src.p, t->rev_wpre.p, t->dir};
-  DevBuf<uint32_t> nitems(t->n_head, s), ipos(t->n_head, s), tot(1, s);
+  PlanShape ps = shape;
+  if (!(t->work_pred.p && t->pred_per_probe > 0)) ps.pred = nullptr;
+  ps.unit = t->pred_per_probe * shape.chunk;
+  DevBuf<uint32_t> nw(t->n_head, s), nb(t->n_head, s), pw(t->n_head, s), pb(t->n_head, s), tot(2, s);
   const int grid = num_sms() * 4;
-  if (t->work_pred.p && t->pred_per_probe > 0)
-    plan_count_pred_kernel<<<grid, 256, 0, s>>>(r, t->n_head, t->work_pred.p, t->pred_per_probe * chunk, nitems.p);
-  else
-    plan_count_kernel<<<grid, 256, 0, s>>>(r, t->n_head, chunk, nitems.p);
+  plan_split_kernel<<<grid, 256, 0, s>>>(t->view(), r, ps, nw.p, nb.p);
   EH_CHECK_LAUNCH();
-  exclusive_scan<uint32_t>(nitems.p, ipos.p, t->n_head, tot.p, s);
-  uint32_t n = 0;
-  EH_CUDA(cudaMemcpyAsync(&n, tot.p, 4, cudaMemcpyDeviceToHost, s));
+  exclusive_scan<uint32_t>(nw.p, pw.p, t->n_head, tot.p, s);
+  exclusive_scan<uint32_t>(nb.p, pb.p, t->n_head, tot.p + 1, s);
+  uint32_t h[2] = {0, 0};
+  EH_CUDA(cudaMemcpyAsync(h, tot.p, 8, cudaMemcpyDeviceToHost, s));
   EH_CUDA(cudaStreamSynchronize(s));
-  plan.items.alloc(n ? n : 1, s);
-  plan.n = n;
-  if (n) {
-    plan_fill_kernel<<<grid, 256, 0, s>>>(r, t->n_head, nitems.p, ipos.p, n, g, plan.items.p);
+  plan.nb = h[1];
+  plan.n = h[0] + h[1];
+  plan.items.alloc(plan.n ? plan.n : 1, s);
+  if (h[1]) {
+    plan_fill_kernel<<<grid, 256, 0, s>>>(r, t->n_head, nb.p, pb.p, h[1], g, plan.items.p);
     EH_CHECK_LAUNCH();
   }
+  if (h[0]) {
+    plan_fill_kernel<<<grid, 256, 0, s>>>(r, t->n_head, nw.p, pw.p, h[0], g, plan.items.p + h[1]);
+    EH_CHECK_LAUNCH();
+  }
+  return 1 + 2 * scan_launches(t->n_head) + (h[0] ? 1 : 0) + (h[1] ? 1 : 0);
 }
 
 // ------------------------------------------------------------------ probes
@@ -521,6 +560,54 @@ __device__ __forceinline__ int stage_set(const TrieView& t, uint32_t hb, uint32_
   return P_GLIST;
 }
 
+// stage_set for a block item: every thread of the block copies, into the
+// block's whole shared region (the caller synchronises the block after).
+__device__ __forceinline__ int stage_set_block(const TrieView& t, uint32_t hb, uint32_t* sm, int cap_words,
+                                               Staged& st) {
+  const uint8_t layout = t.layout[hb];
+  const SetAux a = t.aux[hb];
+  const uint64_t s0 = t.off[hb];
+  const uint32_t len = (uint32_t)(t.off[hb + 1] - s0);
+  if (layout == EH_LAYOUT_RANGE_BITSET) {
+    st.start = a.start;
+    st.n = a.n;
+    if (2 * a.n <= (uint32_t)cap_words) {
+      uint64_t* sw = reinterpret_cast<uint64_t*>(sm);
+      for (uint32_t j = threadIdx.x; j < a.n; j += blockDim.x) sw[j] = __ldg(t.bs_words + a.off + j);
+      st.words = sw;
+      return P_SBITS;
+    }
+    st.words = t.bs_words + a.off;
+    return P_GBITS;
+  }
+  if (layout == EH_LAYOUT_BLOCK_BITSET) {
+    st.ids = t.bb_id + a.off;
+    st.bwords = t.bb_words + 4 * a.off;
+    st.n = a.n;
+    return P_GBLOCK;
+  }
+  st.n = len;
+  if (len <= (uint32_t)cap_words) {
+    for (uint32_t j = threadIdx.x; j < len; j += blockDim.x) sm[j] = __ldg(t.vals + s0 + j);
+    st.list = sm;
+    return P_SLIST;
+  }
+  st.list = t.vals + s0;
+  return P_GLIST;
+}
+
+template <int kMode>
+__device__ __forceinline__ uint64_t rows_of(int mode, const Staged& st, const TrieView& t, const RevView& r,
+                                            uint32_t kb, uint32_t ke, uint32_t long_row, const Sink& sk) {
+  switch (mode) {
+    case P_SBITS: return stream_rows<P_SBITS, kMode>(st, t, r, kb, ke, long_row, sk);
+    case P_GBITS: return stream_rows<P_GBITS, kMode>(st, t, r, kb, ke, long_row, sk);
+    case P_SLIST: return stream_rows<P_SLIST, kMode>(st, t, r, kb, ke, long_row, sk);
+    case P_GLIST: return stream_rows<P_GLIST, kMode>(st, t, r, kb, ke, long_row, sk);
+    default: return stream_rows<P_GBLOCK, kMode>(st, t, r, kb, ke, long_row, sk);
+  }
+}
+
 struct QueryOut {
   uint32_t shard_index, shard_count;  // this launch runs items shard_index + q * shard_count
   uint32_t long_row;                  // size-class boundary of rows (warp-wide vs flattened)
@@ -536,6 +623,8 @@ struct QueryOut {
   int32_t hot[kHot];           // MODE_ANNOT on a symmetric relation: largest sets' head entries, -1 if none
   uint32_t* gsbuf;             // 4-clique: per-warp S buffers in global memory (sets too large for
   uint32_t gcap;               //   shared memory), gcap words each; null: S in shared memory
+  uint32_t n_bitems;           // MODE_COUNT: items[0, n_bitems) are block items, the rest warp items
+  unsigned int* bqueue;        // atomic queue head of the block items
 };
 
 template <int kMode>
@@ -559,13 +648,35 @@ __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict_
   uint32_t* sm = smem + (size_t)wid * cap_words;
   unsigned long long acc = 0;
   uint32_t cur_g = 0xffffffffu;
+  // Block items first (MODE_COUNT only): the block pulls an item, stages its
+  // N(b) across the whole shared region, and its warps take the rows 32 at a
+  // time from a block counter.  Then each warp pulls warp items on its own.
+  __shared__ unsigned int s_q, s_next;
+  const uint32_t nwarps = blockDim.x >> 5;
+  bool block_phase = kMode == MODE_COUNT && out.n_bitems > 0;
+  const uint32_t n_witems = n_items - (kMode == MODE_COUNT ? out.n_bitems : 0u);
   for (;;) {
-    uint32_t q = 0;
-    if (lane == 0) q = atomicAdd(out.queue, 1u);
-    q = __shfl_sync(kFull, q, 0);
-    const uint64_t it64 = (uint64_t)out.shard_index + (uint64_t)q * out.shard_count;
-    if (it64 >= n_items) break;
-    const uint32_t it = (uint32_t)it64;
+    uint32_t it;
+    if (block_phase) {
+      if (threadIdx.x == 0) {
+        s_q = atomicAdd(out.bqueue, 1u);
+        s_next = 0;
+      }
+      __syncthreads();
+      const uint64_t bi64 = (uint64_t)out.shard_index + (uint64_t)s_q * out.shard_count;
+      if (bi64 >= out.n_bitems) {  // the same on every thread of the block
+        block_phase = false;
+        continue;
+      }
+      it = (uint32_t)bi64;
+    } else {
+      uint32_t q = 0;
+      if (lane == 0) q = atomicAdd(out.queue, 1u);
+      q = __shfl_sync(kFull, q, 0);
+      const uint64_t it64 = (uint64_t)out.shard_index + (uint64_t)q * out.shard_count;
+      if (it64 >= n_witems) break;
+      it = (uint32_t)it64 + (kMode == MODE_COUNT ? out.n_bitems : 0u);
+    }
     const Item item = items[it];
     if (item.g != cur_g) {  // flush the running count of the previous graph
       if (lane == 0 && cur_g != 0xffffffffu && acc) atomicAdd(out.total + cur_g, acc);
@@ -585,7 +696,13 @@ __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict_
       sk.b = t.head[item.hb];
     }
     Staged st;
-    const int mode = stage_set(t, item.hb, sm, cap_words, st);
+    int mode;
+    if (block_phase) {
+      mode = stage_set_block(t, item.hb, smem, cap_words * (int)nwarps, st);
+      __syncthreads();
+    } else {
+      mode = stage_set(t, item.hb, sm, cap_words, st);
+    }
     const uint64_t b0 = t.off[item.hb];
     const uint32_t blen = (uint32_t)(t.off[item.hb + 1] - b0);
     if (kMode == MODE_ANNOT && r.dir == DIR_SYM && (mode == P_SLIST || mode == P_SBITS)) {
@@ -608,13 +725,19 @@ __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict_
         __syncwarp();
       }
     }
-    uint64_t c;
-    switch (mode) {
-      case P_SBITS: c = stream_rows<P_SBITS, kMode>(st, t, r, item.kb, item.ke, out.long_row, sk); break;
-      case P_GBITS: c = stream_rows<P_GBITS, kMode>(st, t, r, item.kb, item.ke, out.long_row, sk); break;
-      case P_SLIST: c = stream_rows<P_SLIST, kMode>(st, t, r, item.kb, item.ke, out.long_row, sk); break;
-      case P_GLIST: c = stream_rows<P_GLIST, kMode>(st, t, r, item.kb, item.ke, out.long_row, sk); break;
-      default: c = stream_rows<P_GBLOCK, kMode>(st, t, r, item.kb, item.ke, out.long_row, sk); break;
+    uint64_t c = 0;
+    if (block_phase) {
+      for (;;) {
+        uint32_t batch = 0;
+        if (lane == 0) batch = atomicAdd(&s_next, 1u);
+        batch = __shfl_sync(kFull, batch, 0);
+        const uint64_t k0 = (uint64_t)item.kb + 32ull * batch;
+        if (k0 >= item.ke) break;
+        const uint32_t k1 = k0 + 32 < (uint64_t)item.ke ? (uint32_t)(k0 + 32) : item.ke;
+        c += rows_of<kMode>(mode, st, t, r, (uint32_t)k0, k1, out.long_row, sk);
+      }
+    } else {
+      c = rows_of<kMode>(mode, st, t, r, item.kb, item.ke, out.long_row, sk);
     }
     c = warp_sum(c);
     if (kMode == MODE_ANNOT && sk.wcnt) {  // flush the item's per-element counts
@@ -627,12 +750,13 @@ __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict_
     if (kMode == MODE_ANNOT && r.dir == DIR_SYM && lane == 0 && c) atomicAdd(out.annot + item.hb, 2ull * c);
     if (out.item_counts && lane == 0) out.item_counts[it] = c * out.count_mult;
     acc += c;
-    __syncwarp();  // the staged region is reused by the next item
-    if (out.records && lane == 0) {
+    if (block_phase) __syncthreads();  // every warp is done with the staged set
+    else __syncwarp();                 // the staged region is reused by the next item
+    if (out.records && (block_phase ? threadIdx.x == 0 : lane == 0)) {
       const long long t1 = clock64();
-      const uint32_t len = (uint32_t)(t.off[item.hb + 1] - t.off[item.hb]);
+      const uint32_t len = blen;
       const uint64_t pairs = r.rev_wpre[item.ke] - r.rev_wpre[item.kb];
-      const uint32_t first = t.vals[t.off[item.hb]], last = t.vals[t.off[item.hb + 1] - 1];
+      const uint32_t first = t.vals[b0], last = t.vals[b0 + len - 1];
       float* rec = out.records + 8 * (size_t)it;
       rec[0] = (float)len;
       rec[1] = (float)pairs;
@@ -641,7 +765,7 @@ __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict_
       rec[4] = (float)t.layout[item.hb];
       rec[5] = (float)mode;
       rec[6] = __uint_as_float(item.hb);  // set id, bit pattern
-      rec[7] = (float)(t1 - t0);
+      rec[7] = (float)(t1 - t0) * (block_phase ? (float)nwarps : 1.f);  // warp-cycles
     }
   }
   if (lane == 0 && cur_g != 0xffffffffu && acc) atomicAdd(out.total + cur_g, acc);
@@ -653,9 +777,14 @@ __global__ void EH_TRI_LAUNCH_BOUNDS triangle_kernel(const TrieView* __restrict_
 }
 
 // ------------------------------------------------------------ 4-clique
-// For every row a->b (UP / DOWN / SYM-oriented): S = candidates(a,b) ∩ N(b)
-// is materialised in the warp's shared region, then for each c in S the
-// elements of S on the far side of c are probed in N(c).
+// For every row a->b: S = candidates(a,b) ∩ N(b) is materialised in the
+// warp's shared region, then for each c in S the elements d of S are probed
+// in N(c).  On an up- or down-oriented relation (or a symmetric one, rows
+// a<b) only the d on the far side of c can close a 4-clique; on a general
+// relation (self-loops, rows in both directions that are not symmetric) the
+// candidates are the whole N(a) and every d of S is probed: the count is the
+// number of assignments (a,b,c,d) with all six rows present, which is what
+// the reference's N-way loop nest counts (TrieBuilder.cpp:276-348).
 __device__ __forceinline__ uint32_t probe_global_set(const TrieView& t, uint32_t hc, uint32_t w) {
   const uint8_t layout = t.layout[hc];
   const SetAux a = t.aux[hc];
@@ -694,6 +823,7 @@ __device__ uint64_t clique_rows(const Staged& st, const TrieView& t, const RevVi
                                 uint32_t* sbuf, uint32_t cap, const uint32_t* sel, uint32_t wb) {
   const uint32_t lane = lane_id();
   const bool up = r.dir != DIR_DOWN;
+  const bool general = r.dir == DIR_GENERAL;
   uint64_t cnt = 0;
   for (uint32_t k = kb; k < ke; k++) {
     uint32_t wab = 0;
@@ -726,7 +856,7 @@ __device__ uint64_t clique_rows(const Staged& st, const TrieView& t, const RevVi
       const uint32_t c = sbuf[i];
       const int32_t hc = __ldg(t.head_index + c);
       if (hc < 0) continue;
-      const uint32_t jb = up ? i + 1 : 0, je = up ? ns : i;
+      const uint32_t jb = general ? 0 : (up ? i + 1 : 0), je = general ? ns : (up ? ns : i);
       if (sel && r.dir == DIR_SYM) {
         const uint32_t wabc = wab + sel_bit(sel, c);
         for (uint32_t j = jb + lane; j < je; j += 32)
@@ -769,6 +899,8 @@ __global__ void EH_TRI_LAUNCH_BOUNDS clique4_kernel(const TrieView* __restrict__
     }
     const TrieView t = views[item.g];
     const RevView r = revs[item.g];
+    long long t0 = 0;
+    if (out.records && lane == 0) t0 = clock64();
     Staged st;
     const int mode = stage_set(t, item.hb, sm, half, st);
     const uint32_t wb = out.sel ? sel_bit(out.sel, t.head[item.hb]) : 0u;
@@ -782,6 +914,21 @@ __global__ void EH_TRI_LAUNCH_BOUNDS clique4_kernel(const TrieView* __restrict__
     }
     acc += warp_sum(c);
     __syncwarp();
+    if (out.records && lane == 0) {  // the same record as the triangle kernel's
+      const long long t1 = clock64();
+      const uint64_t b0 = t.off[item.hb];
+      const uint32_t len = (uint32_t)(t.off[item.hb + 1] - b0);
+      const uint32_t first = t.vals[b0], last = t.vals[b0 + len - 1];
+      float* rec = out.records + 8 * (size_t)it;
+      rec[0] = (float)len;
+      rec[1] = (float)(r.rev_wpre[item.ke] - r.rev_wpre[item.kb]);
+      rec[2] = (float)len / (float)(last - first + 1);
+      rec[3] = (float)(last - first);
+      rec[4] = (float)t.layout[item.hb];
+      rec[5] = (float)mode;
+      rec[6] = __uint_as_float(item.hb);
+      rec[7] = (float)(t1 - t0);
+    }
   }
   if (lane == 0 && cur_g != 0xffffffffu && acc) atomicAdd(out.total + cur_g, acc);
 }
@@ -868,6 +1015,7 @@ struct Launch {
 struct Prepared {
   DevBuf<Item> items;
   uint32_t n_items = 0;
+  uint32_t n_bitems = 0;  // items[0, n_bitems) are block items
   uint64_t pairs = 0;
   DevBuf<TrieView> dv;
   DevBuf<RevView> dr;
@@ -916,44 +1064,11 @@ static void hot_sets(eh_context* ctx, const eh_trie* t, int32_t* hot) {
 }
 
 static void prepare(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query, ExecParams ep, bool annot,
-                    Prepared& P) {
+                    Prepared& P, bool block_items = false) {
   cudaStream_t s = ctx->stream;
   P.query = query;
   P.annot = annot;
-  std::vector<Plan> plans(n);
-  uint32_t total_items = 0;
-  uint64_t pairs = 0;
-  for (uint32_t g = 0; g < n; g++) {
-    build_plan(ctx, tries[g], ep.chunk, g, plans[g]);
-    P.plan_launches += plans[g].n ? 2 : 1;
-    total_items += plans[g].n;
-    pairs += tries[g]->rev_pairs;
-  }
-  P.n_items = total_items;
-  P.pairs = pairs;
-  if (n == 1) {
-    P.items = std::move(plans[0].items);
-  } else {
-    P.items.alloc(total_items ? total_items : 1, s);
-    uint32_t o = 0;
-    for (uint32_t g = 0; g < n; g++) {
-      if (plans[g].n)
-        EH_CUDA(cudaMemcpyAsync(P.items.p + o, plans[g].items.p, plans[g].n * sizeof(Item), cudaMemcpyDeviceToDevice,
-                                s));
-      o += plans[g].n;
-    }
-  }
-  std::vector<TrieView> hv(n);
-  std::vector<RevView> hr(n);
-  for (uint32_t g = 0; g < n; g++) {
-    hv[g] = tries[g]->view();
-    hr[g] = rev_view(tries[g]);
-  }
-  P.dv.alloc(n, s);
-  P.dr.alloc(n, s);
-  P.q.alloc(2, s);
-  EH_CUDA(cudaMemcpyAsync(P.dv.p, hv.data(), n * sizeof(TrieView), cudaMemcpyHostToDevice, s));
-  EH_CUDA(cudaMemcpyAsync(P.dr.p, hr.data(), n * sizeof(RevView), cudaMemcpyHostToDevice, s));
+  // the launch shape first: the plan's classes depend on the staging capacity
   // the annotated pass stages more of N(b) by default: its matched elements
   // then count in shared memory (measured on Chung-Lu 2^23: 2048 words per
   // warp 234 ms, 1024 245 ms)
@@ -972,6 +1087,50 @@ static void prepare(eh_context* ctx, const eh_trie* const* tries, uint32_t n, in
       P.smem = (size_t)ep.smem_words * 4 * ep.warps;
     }
   }
+  // block items only for the plain triangle COUNT
+  const bool blocks = block_items && query == EH_QUERY_TRIANGLE && !annot && ep.warps > 1 && !ep.no_block_items;
+  PlanShape shape{ep.chunk, nullptr, 0.0, (uint32_t)ep.smem_words,
+                   blocks ? (uint32_t)ep.smem_words * (uint32_t)ep.warps : 0u, (uint32_t)ep.warps};
+  std::vector<Plan> plans(n);
+  uint32_t total_items = 0, total_b = 0;
+  uint64_t pairs = 0;
+  for (uint32_t g = 0; g < n; g++) {
+    P.plan_launches += build_plan(ctx, tries[g], shape, g, plans[g]);
+    total_items += plans[g].n;
+    total_b += plans[g].nb;
+    pairs += tries[g]->rev_pairs;
+  }
+  P.n_items = total_items;
+  P.n_bitems = total_b;
+  P.pairs = pairs;
+  if (n == 1) {
+    P.items = std::move(plans[0].items);
+  } else {
+    // every graph's block items, then every graph's warp items
+    P.items.alloc(total_items ? total_items : 1, s);
+    uint32_t ob = 0, ow = total_b;
+    for (uint32_t g = 0; g < n; g++) {
+      const uint32_t nb = plans[g].nb, nw = plans[g].n - plans[g].nb;
+      if (nb)
+        EH_CUDA(cudaMemcpyAsync(P.items.p + ob, plans[g].items.p, nb * sizeof(Item), cudaMemcpyDeviceToDevice, s));
+      if (nw)
+        EH_CUDA(cudaMemcpyAsync(P.items.p + ow, plans[g].items.p + nb, nw * sizeof(Item), cudaMemcpyDeviceToDevice,
+                                s));
+      ob += nb;
+      ow += nw;
+    }
+  }
+  std::vector<TrieView> hv(n);
+  std::vector<RevView> hr(n);
+  for (uint32_t g = 0; g < n; g++) {
+    hv[g] = tries[g]->view();
+    hr[g] = rev_view(tries[g]);
+  }
+  P.dv.alloc(n, s);
+  P.dr.alloc(n, s);
+  P.q.alloc(2, s);
+  EH_CUDA(cudaMemcpyAsync(P.dv.p, hv.data(), n * sizeof(TrieView), cudaMemcpyHostToDevice, s));
+  EH_CUDA(cudaMemcpyAsync(P.dr.p, hr.data(), n * sizeof(RevView), cudaMemcpyHostToDevice, s));
   const void* kfn;
   if (query == EH_QUERY_CLIQUE4) {
     set_smem_attr(clique4_kernel, P.smem);
@@ -984,7 +1143,8 @@ static void prepare(eh_context* ctx, const eh_trie* const* tries, uint32_t n, in
     kfn = (const void*)triangle_kernel<MODE_COUNT>;
   }
   const int per_sm = blocks_per_sm(kfn, P.threads, P.smem);
-  P.grid = std::max(1, std::min(num_sms() * per_sm, (int)((total_items + ep.warps - 1) / ep.warps)));
+  const uint64_t units = (uint64_t)total_b + (total_items - total_b + ep.warps - 1) / ep.warps;
+  P.grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms() * per_sm, units));
   if (annot && n == 1 && tries[0]->dir == DIR_SYM) hot_sets(ctx, tries[0], P.hot);
   if (query == EH_QUERY_CLIQUE4 && ep.s_cap) {
     // one S buffer per resident warp, at most 2 GiB in all
@@ -1005,6 +1165,8 @@ static void launch(eh_context* ctx, Prepared& P, unsigned long long* d_total, un
   EH_CUDA(cudaMemsetAsync(P.q.p, 0, 8, s));
   const ExecParams& ep = P.ep;
   QueryOut out{ep.shard_index, ep.shard_count, ep.long_row, d_total, d_annot, d_records, P.q.p};
+  out.n_bitems = P.n_bitems;
+  out.bqueue = P.q.p + 1;
   out.sel = P.sel;
   for (int k = 0; k < kHot; k++) out.hot[k] = P.hot[k];
   out.gsbuf = ep.s_cap ? P.gs.p : nullptr;
@@ -1040,7 +1202,7 @@ static Launch run_plans(eh_context* ctx, const eh_trie* const* tries, uint32_t n
   cudaStream_t s = ctx->stream;
   Launch L;
   Prepared P;
-  prepare(ctx, tries, n, query, ep, annot, P);
+  prepare(ctx, tries, n, query, ep, annot, P, true);
   P.sel = sel;
   L.launches = P.plan_launches;
   *n_items_out = P.n_items;
@@ -1175,10 +1337,6 @@ void query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t 
     EH_REQUIRE(tries[g] != nullptr, EH_ERR_INVALID, "null trie");
     EH_REQUIRE(tries[g]->ctx == ctx, EH_ERR_INVALID, "trie belongs to another context");
   }
-  if (query == EH_QUERY_CLIQUE4)
-    for (uint32_t g = 0; g < n; g++)
-      EH_REQUIRE(tries[g]->dir != DIR_GENERAL || tries[g]->rows == 0, EH_ERR_UNSUPPORTED,
-                 "4-clique needs a relation that is up-, down-oriented or symmetric");
   ExecParams ep = exec_params(cfg);
   if (query == EH_QUERY_CLIQUE4) {
     uint32_t mx = 0;
@@ -1207,10 +1365,15 @@ void query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t 
     EH_REQUIRE(n == 1, EH_ERR_UNSUPPORTED, "batched lollipop/barbell is not supported");
     const eh_trie* t = tries[0];
     EH_REQUIRE(ep.shard_count == 1, EH_ERR_UNSUPPORTED, "lollipop/barbell run unsharded");
+    float* recp = nullptr;
+    if (record) {  // the annotated triangle pass's items (the root bag is not logged)
+      rec.alloc(8 * (t->n_head + t->rev_pairs / ep.chunk + 16), s);
+      recp = rec.p;
+    }
     DevBuf<unsigned long long> T(t->n_head ? t->n_head : 1, s), dummy(1, s);
     EH_CUDA(cudaMemsetAsync(T.p, 0, (t->n_head ? t->n_head : 1) * 8, s));
     EH_CUDA(cudaMemsetAsync(dummy.p, 0, 8, s));
-    L = run_plans(ctx, tries, 1, EH_QUERY_TRIANGLE, ep, true, dummy.p, T.p, nullptr, &items, &pairs);
+    L = run_plans(ctx, tries, 1, EH_QUERY_TRIANGLE, ep, true, dummy.p, T.p, recp, &items, &pairs);
     L.launches += root_bag(ctx, t, query, T.p, nullptr, total.p);
   }
   std::vector<unsigned long long> h(n);
@@ -1330,8 +1493,6 @@ void query_count_select(eh_context* ctx, const eh_trie* t, int query, uint32_t v
   EH_REQUIRE(ep.shard_count == 1, EH_ERR_UNSUPPORTED, "selection plans run unsharded");
   const bool clique = query == EH_QUERY_CLIQUE4_SEL;
   if (clique) {
-    EH_REQUIRE(t->dir != DIR_GENERAL || t->rows == 0, EH_ERR_UNSUPPORTED,
-               "4-clique needs a relation that is up-, down-oriented or symmetric");
     size_clique_staging(ep, t->info.max_set);
   }
   EH_CUDA(cudaEventRecord(ctx->ev0, s));
@@ -1571,8 +1732,6 @@ void query_count_in_scratch(eh_context* ctx, const eh_trie* t, int query, const 
   EH_REQUIRE(ep.shard_count == 1, EH_ERR_UNSUPPORTED, "the allocation-free path runs unsharded");
   const bool clique = query == EH_QUERY_CLIQUE4;
   if (clique) {
-    EH_REQUIRE(t->dir != DIR_GENERAL || t->rows == 0, EH_ERR_UNSUPPORTED,
-               "4-clique needs a relation that is up-, down-oriented or symmetric");
     size_clique_staging(ep, t->info.max_set);
   }
   // launch shape and shared memory, checked before anything is launched
@@ -1702,8 +1861,6 @@ eh_batch* batch_create(eh_context* ctx, const eh_trie* const* tries, uint32_t n,
   for (uint32_t g = 0; g < n; g++) {
     EH_REQUIRE(tries[g] && tries[g]->ctx == ctx, EH_ERR_INVALID, "null trie or trie of another context");
     if (query == EH_QUERY_CLIQUE4) {
-      EH_REQUIRE(tries[g]->dir != DIR_GENERAL || tries[g]->rows == 0, EH_ERR_UNSUPPORTED,
-                 "4-clique needs a relation that is up-, down-oriented or symmetric");
       mx = std::max(mx, tries[g]->info.max_set);
     }
   }
@@ -1714,7 +1871,7 @@ eh_batch* batch_create(eh_context* ctx, const eh_trie* const* tries, uint32_t n,
     b->n = n;
     b->query = query;
     for (uint32_t g = 0; g < n; g++) b->dirs.push_back(tries[g]->dir);
-    prepare(ctx, tries, n, query, ep, false, b->P);
+    prepare(ctx, tries, n, query, ep, false, b->P, true);
     b->total.alloc(n, s);
     EH_CUDA(cudaMallocHost((void**)&b->host, n * sizeof(unsigned long long)));
     EH_CUDA(cudaStreamSynchronize(s));

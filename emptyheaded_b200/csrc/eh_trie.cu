@@ -467,8 +467,17 @@ void trie_layout(eh_context* ctx, eh_trie* t, const eh_layout_config* cfg) {
   const uint32_t n_sets = t->n_head + 1;
   const int policy = cfg ? cfg->policy : EH_POLICY_HEURISTIC;
   const int forced = cfg ? cfg->forced_layout : EH_LAYOUT_UINTEGER;
-  EH_REQUIRE(policy == EH_POLICY_HEURISTIC || policy == EH_POLICY_LEARNED || policy == EH_POLICY_FORCED,
+  EH_REQUIRE(policy == EH_POLICY_HEURISTIC || policy == EH_POLICY_LEARNED || policy == EH_POLICY_FORCED ||
+                 policy == EH_POLICY_EXPLICIT,
              EH_ERR_INVALID, "unknown layout policy");
+  if (policy == EH_POLICY_EXPLICIT) {
+    EH_REQUIRE(cfg->layouts != nullptr || t->n_head == 0, EH_ERR_INVALID, "explicit layout policy needs layouts");
+    for (uint32_t i = 0; i < t->n_head; i++) {
+      const uint8_t l = cfg->layouts[i];
+      EH_REQUIRE(l == EH_LAYOUT_UINTEGER || l == EH_LAYOUT_RANGE_BITSET || l == EH_LAYOUT_BLOCK_BITSET,
+                 EH_ERR_INVALID, "unknown layout in the explicit assignment");
+    }
+  }
   EH_REQUIRE(forced == EH_LAYOUT_UINTEGER || forced == EH_LAYOUT_RANGE_BITSET || forced == EH_LAYOUT_BLOCK_BITSET,
              EH_ERR_INVALID, "unknown forced layout");
   TracePhase ph("layout.choose", s);
@@ -477,6 +486,10 @@ void trie_layout(eh_context* ctx, eh_trie* t, const eh_layout_config* cfg) {
   layout_heuristic_kernel<<<num_sms() * 4, 256, 0, s>>>(set_src(t), n_sets, policy, forced, max_words,
                                                          t->layout.p);
   EH_CHECK_LAUNCH();
+  if (policy == EH_POLICY_EXPLICIT && t->n_head) {
+    EH_CUDA(cudaMemcpyAsync(t->layout.p, cfg->layouts, t->n_head, cudaMemcpyHostToDevice, s));
+    EH_CUDA(cudaStreamSynchronize(s));  // the host array may go away after the call
+  }
   t->work_pred.release();
   t->pred_per_probe = 0;
   if (policy == EH_POLICY_LEARNED) {

@@ -38,8 +38,10 @@ def set_features(head_len, rng, pairs, layout):
     return f
 
 
-def profile(E, trie, reps=2):
-    """Per-set cycles under each layout.  Returns (len, range, pairs,
+def profile(E, trie, reps=2, query="triangle"):
+    """Per-set cycles of `query`'s intersection kernel under each layout
+    (the triangle or 4-clique kernel; for lollipop / barbell, the annotated
+    triangle pass that dominates them).  Returns (len, range, pairs,
     cycles[layout] with NaN where the layout was not admissible, base
     heuristic layout)."""
     head, off, vals, heur = trie.export()
@@ -63,7 +65,7 @@ def profile(E, trie, reps=2):
         _, _, _, lay = trie.export()
         acc = np.zeros(n)
         for _ in range(reps):
-            trie.count("triangle", record=True)
+            trie.count(query, record=True)
             rec = E.timing_records(trie.ctx)
             hb = rec[:, 6].view(np.uint32).astype(np.int64)
             acc += np.bincount(hb, weights=rec[:, 7].astype(np.float64), minlength=n)
@@ -164,13 +166,25 @@ def evaluate(E, model, prof):
     }
 
 
-def train_from_trie(E, trie, passes=2, epochs=60):
-    """Profile `trie`, train the cost model on the logs, evaluate it.
-    Returns (model, info)."""
-    prof = profile(E, trie, reps=passes)
+def best_layouts(prof):
+    """The per-set exhaustive search's assignment: each staged set's
+    cheapest admissible layout by the profiled cycles, the density rule for
+    the sets no plan stages (EH_POLICY_EXPLICIT takes it)."""
+    C = np.stack([prof["cycles"][L] for L in LAYOUTS], 1)
+    C = np.where(np.isfinite(C) & (C > 0), C, np.inf)
+    pick = np.asarray(LAYOUTS, np.uint8)[np.argmin(C, 1)]
+    staged = (prof["pairs"] > 0) & np.isfinite(C.min(1))
+    return np.where(staged, pick, prof["heuristic"].astype(np.uint8)).astype(np.uint8)
+
+
+def train_from_trie(E, trie, passes=2, epochs=60, query="triangle", prof=None):
+    """Profile `trie` (or take its profile), train the cost model on the
+    logs, evaluate it on the same logs.  Returns (model, info, profile)."""
+    prof = prof if prof is not None else profile(E, trie, reps=passes, query=query)
     x, y = dataset(prof)
     model, losses = train(E, x, y, ctx=trie.ctx, epochs=epochs)
     info = evaluate(E, model, prof)
     info["train_rows"] = int(len(x))
     info["final_loss"] = float(np.mean(losses[-20:])) if losses else None
-    return model, info
+    info["query"] = query
+    return model, info, prof

@@ -45,8 +45,11 @@ enum {
  *   (layouts/hybrid.hpp:103-111, utils/common.hpp:60-66).
  * LEARNED: the cost model loaded with eh_trie_build (falls back to the
  *   heuristic where the model abstains).
- * FORCED: every set gets eh_layout_config.forced_layout. */
-enum { EH_POLICY_HEURISTIC = 0, EH_POLICY_LEARNED = 1, EH_POLICY_FORCED = 2 };
+ * FORCED: every set gets eh_layout_config.forced_layout.
+ * EXPLICIT: level-1 set i gets eh_layout_config.layouts[i] (an assignment
+ *   found elsewhere, e.g. the per-set exhaustive search that bounds every
+ *   layout policy); the head set keeps the density rule. */
+enum { EH_POLICY_HEURISTIC = 0, EH_POLICY_LEARNED = 1, EH_POLICY_FORCED = 2, EH_POLICY_EXPLICIT = 3 };
 
 /* Named generic-join plans executed as one device bag each. */
 enum {
@@ -145,6 +148,7 @@ typedef struct {
    * heuristic layout.  0: no cap for FORCED; LEARNED always applies the
    * per-element bound. */
   uint64_t max_bitset_bytes;
+  const uint8_t* layouts; /* EH_POLICY_EXPLICIT: host array, one EH_LAYOUT_* per level-1 set (n_head) */
 } eh_layout_config;
 
 typedef struct {
@@ -226,6 +230,10 @@ typedef struct {
   int record_timings;    /* 1: log per-item device time for the cost model */
   int shard_index;       /* run work items i with i % shard_count == shard_index */
   int shard_count;       /* 0 or 1: all items (multi-GPU ranks split the plan) */
+  int no_block_items;    /* 1: stage every N(b) in one warp's region; 0: an N(b)
+                            too large for a warp's region but not for the
+                            block's is staged block-wide and all the block's
+                            warps share its rows (triangle COUNT) */
 } eh_exec_config;
 
 typedef struct {

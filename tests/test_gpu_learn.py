@@ -2,10 +2,14 @@
 
 The engine logs per-item device cycles; profiling every set under each
 layout is an exhaustive per-set layout search.  The MLP, trained on those
-logs by the engine's own kernels, must (1) predict the per-set cost within a
-bounded error, (2) pick layouts whose measured cost is closer to the
+logs by the engine's own kernels, is judged on a graph it was not trained on
+(a different seed and scale): it must (1) predict the per-set cost within a
+bounded error there, (2) pick layouts whose measured cost is closer to the
 exhaustive optimum than the heuristic's (lower regret), and (3) change only
-speed: the count is the same under the learned layouts."""
+speed: the count is the same under the learned layouts, under the
+exhaustive search's own assignment (EH_POLICY_EXPLICIT), and for a model
+trained on the 4-clique kernel's logs."""
+import numpy as np
 import pytest
 
 from emptyheaded_b200 import learn, workloads
@@ -13,15 +17,35 @@ from emptyheaded_b200 import learn, workloads
 pytestmark = pytest.mark.gpu
 
 
-def test_learned_layouts_beat_heuristic_regret(eh):
-    t = workloads.build_rmat_trie(eh, 18, 7)
+def test_learned_layouts_beat_heuristic_regret_held_out(eh):
+    train = workloads.build_rmat_trie(eh, 17, 7)
+    model, info_in, _ = learn.train_from_trie(eh, train, passes=2, epochs=25)
+    train.free()
+    t = workloads.build_rmat_trie(eh, 18, 8)
     want = t.count("triangle")
-    model, info = learn.train_from_trie(eh, t, passes=2, epochs=25)
-    assert info["median_abs_pct_error"] < 25.0, info
-    assert info["regret_learned_pct"] < info["regret_heuristic_pct"], info
+    prof = learn.profile(eh, t, reps=2)
+    info = learn.evaluate(eh, model, prof)
+    assert info["median_abs_pct_error"] < 30.0, (info, info_in)
+    assert info["regret_learned_pct"] < info["regret_heuristic_pct"], (info, info_in)
     t.relayout(policy=eh.LEARNED, model=model)
     assert t.count("triangle") == want
     h = t.info()
     assert h["n_uinteger"] + h["n_range_bitset"] + h["n_block_bitset"] == h["n_head"]
+    best = learn.best_layouts(prof)
+    t.relayout(policy=eh.EXPLICIT, layouts=best)
+    assert t.count("triangle") == want
+    _, _, _, lay = t.export()
+    np.testing.assert_array_equal(lay, best)
+    t.free()
+    model.free()
+
+
+def test_model_trained_on_clique4_logs(eh):
+    t = workloads.build_rmat_trie(eh, 15, 42)
+    want = t.count("clique4")
+    model, info, prof = learn.train_from_trie(eh, t, passes=1, epochs=20, query="clique4")
+    assert info["sets_staged"] > 0 and info["query"] == "clique4"
+    t.relayout(policy=eh.LEARNED, model=model)
+    assert t.count("clique4") == want
     t.free()
     model.free()

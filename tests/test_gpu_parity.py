@@ -185,6 +185,7 @@ def test_general_direction_relation(eh, oracle):
     for _, policy, forced in POLICIES:
         t = eh.Trie(s, d, policy=policy, forced=forced)
         assert t.count("triangle") == o.triangle()
+        assert t.count("clique4") == o.clique4()
         assert t.count("lollipop") == o.lollipop()
         assert t.count("barbell") == o.barbell()
         np.testing.assert_array_equal(t.triangle_annotation(), o.triangle_per_vertex())

@@ -19,7 +19,7 @@ def test_shards_sum_to_the_count(eh, oracle):
     for world in (2, 3, 8):
         for q in want:
             assert _shares(t, q, world) == want[q], (q, world)
-    model, info = learn.train_from_trie(eh, t, passes=1, epochs=20)
+    model, info, _ = learn.train_from_trie(eh, t, passes=1, epochs=20)
     t.relayout(policy=eh.LEARNED, model=model)
     for world in (2, 3, 8):
         for q in want:
