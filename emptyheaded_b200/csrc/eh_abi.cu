@@ -200,6 +200,10 @@ eh_status eh_context_destroy(eh_context* ctx) {
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->ev2) cudaEventDestroy(ctx->ev2);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->copy_stream) {
+      cudaStreamSynchronize(ctx->copy_stream);
+      cudaStreamDestroy(ctx->copy_stream);
+    }
     trim_device_pool(ctx->device);  // return the pool's unused blocks to the driver
     delete ctx;
   });
@@ -649,24 +653,7 @@ eh_status eh_query_count_host_csr(eh_context* ctx, const uint32_t* head, uint32_
     need(t.rows < (1ull << 32), "tries hold fewer than 2^32 rows");
     need(off[0] == 0, "off[0] must be 0");
     TracePhase all("host_csr.total", s);
-    {
-      TracePhase ph("host_csr.h2d", s);
-      t.head.alloc(n_head ? n_head : 1, s);
-      t.off.alloc(n_head + 1, s);
-      t.vals.alloc(t.rows ? t.rows : 1, s);
-      if (n_head) EH_CUDA(cudaMemcpyAsync(t.head.p, head, n_head * 4, cudaMemcpyHostToDevice, s));
-      EH_CUDA(cudaMemcpyAsync(t.off.p, off, (n_head + 1) * 8, cudaMemcpyHostToDevice, s));
-      if (t.rows) EH_CUDA(cudaMemcpyAsync(t.vals.p, vals, t.rows * 4, cudaMemcpyHostToDevice, s));
-    }
-    {
-      TracePhase ph("host_csr.domain", s);
-      // the value domain bounds head_index[]: take it from the data, never
-      // from the caller's n_nodes alone
-      const uint32_t mh = n_head ? max_u32(t.head.p, n_head, s) : 0;
-      const uint32_t mv = t.rows ? max_u32(t.vals.p, t.rows, s) : 0;
-      t.n_nodes = (n_head || t.rows) ? std::max(n_nodes, std::max(mh, mv) + 1) : 0;
-    }
-    trie_build_from_csr(ctx, &t);
+    trie_build_from_host_csr(ctx, &t, head, off, vals, n_nodes);
     trie_layout(ctx, &t, cfg);
     TracePhase ph("host_csr.query", s);
     query_count(ctx, &t, query, ecfg, result, stats);

@@ -8,6 +8,7 @@
 struct eh_context {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // host-to-device copies overlapped with work on `stream`
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
   // per-item timing records of the last recorded query (8 floats each)
   std::vector<float> timing_records;
@@ -134,6 +135,9 @@ void trie_build(eh_context* ctx, const uint32_t* col0, const uint32_t* col1, uin
                 eh_trie* t);
 void trie_build_from_csr(eh_context* ctx, eh_trie* t);  // head/off/vals already set
 void trie_build_reverse(eh_context* ctx, eh_trie* t);   // dir + reverse level
+// head/off/vals from host memory, the vals copy overlapped with the row work
+void trie_build_from_host_csr(eh_context* ctx, eh_trie* t, const uint32_t* head, const uint64_t* off,
+                              const uint32_t* vals, uint32_t n_nodes_hint);
 void trie_layout(eh_context* ctx, eh_trie* t, const eh_layout_config* cfg);
 void trie_set_bytes(const eh_trie* t, uint32_t set_index, std::vector<uint8_t>& out, uint8_t* layout);
 // the reference's on-disk format (eh_disk.cu)

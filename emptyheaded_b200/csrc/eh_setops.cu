@@ -12,8 +12,8 @@
 //                    lane probes the larger set by branch-free binary search
 //                    (shared memory when it fits)
 //   X ∩ bitset       the other set is streamed, one word test per element
-//   bitset ∩ bitset  128-bit loads of both word ranges over their overlap,
-//                    AND + popcount, warp reduction
+//   bitset ∩ bitset  one 64-bit word of each range per lane over their
+//                    overlap (coalesced), AND + popcount, warp reduction
 //   X ∩ block        streamed elements probe the block ids
 // Materialized results are written in increasing order (ballot compaction
 // of the streamed side, or bit order of the AND-ed words).

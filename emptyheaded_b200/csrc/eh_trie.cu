@@ -513,45 +513,56 @@ void trie_layout(eh_context* ctx, eh_trie* t, const eh_layout_config* cfg) {
   update_bytes(t);
 }
 
-void trie_build_from_csr(eh_context* ctx, eh_trie* t) {
+// value -> head position over the value domain [0, n_nodes)
+static void build_head_index(eh_context* ctx, eh_trie* t) {
+  cudaStream_t s = ctx->stream;
+  t->head_index.alloc(t->n_nodes ? t->n_nodes : 1, s);
+  EH_CUDA(cudaMemsetAsync(t->head_index.p, 0xff, (size_t)(t->n_nodes ? t->n_nodes : 1) * 4, s));
+  if (t->n_head) {
+    head_index_kernel<<<num_sms() * 8, 256, 0, s>>>(t->head.p, t->n_head, t->head_index.p);
+    EH_CHECK_LAUNCH();
+  }
+}
+
+// wedges per head entry, their total, the largest set, sum of squared sizes
+static void build_stats(eh_context* ctx, eh_trie* t) {
   cudaStream_t s = ctx->stream;
   const int grid = num_sms() * 8;
+  t->wedges.alloc(t->n_head ? t->n_head : 1, s);
+  DevBuf<uint64_t> tot(1, s);
+  if (t->n_head) {
+    wedge_kernel<<<grid, 256, 0, s>>>(t->view(), t->wedges.p);
+    EH_CHECK_LAUNCH();
+    DevBuf<uint64_t> scratch(t->n_head, s);
+    exclusive_scan<uint64_t>(t->wedges.p, scratch.p, t->n_head, tot.p, s);
+    EH_CUDA(cudaMemcpyAsync(&t->total_wedges, tot.p, 8, cudaMemcpyDeviceToHost, s));
+  }
+  EH_CUDA(cudaStreamSynchronize(s));
+  t->info.rows = t->rows;
+  t->info.n_head = t->n_head;
+  t->info.n_nodes = t->n_nodes;
+  uint32_t mx = 0;
+  t->sum_sq_deg = 0;
+  if (t->n_head) {
+    DevBuf<unsigned long long> red(2, s);
+    EH_CUDA(cudaMemsetAsync(red.p, 0, 16, s));
+    set_size_stats_kernel<<<grid, 256, 0, s>>>(t->off.p, t->n_head, red.p);
+    EH_CHECK_LAUNCH();
+    unsigned long long h[2];
+    EH_CUDA(cudaMemcpyAsync(h, red.p, 16, cudaMemcpyDeviceToHost, s));
+    EH_CUDA(cudaStreamSynchronize(s));
+    mx = (uint32_t)h[0];
+    t->sum_sq_deg = h[1];
+  }
+  t->info.max_set = mx;
+}
+
+void trie_build_from_csr(eh_context* ctx, eh_trie* t) {
+  cudaStream_t s = ctx->stream;
   {
     TracePhase ph("build.index+stats", s);
-    t->head_index.alloc(t->n_nodes ? t->n_nodes : 1, s);
-    EH_CUDA(cudaMemsetAsync(t->head_index.p, 0xff, (size_t)(t->n_nodes ? t->n_nodes : 1) * 4, s));
-    if (t->n_head) {
-      head_index_kernel<<<grid, 256, 0, s>>>(t->head.p, t->n_head, t->head_index.p);
-      EH_CHECK_LAUNCH();
-    }
-    t->wedges.alloc(t->n_head ? t->n_head : 1, s);
-    DevBuf<uint64_t> tot(1, s);
-    if (t->n_head) {
-      wedge_kernel<<<grid, 256, 0, s>>>(t->view(), t->wedges.p);
-      EH_CHECK_LAUNCH();
-      DevBuf<uint64_t> scratch(t->n_head, s);
-      exclusive_scan<uint64_t>(t->wedges.p, scratch.p, t->n_head, tot.p, s);
-      EH_CUDA(cudaMemcpyAsync(&t->total_wedges, tot.p, 8, cudaMemcpyDeviceToHost, s));
-    }
-    EH_CUDA(cudaStreamSynchronize(s));
-    t->info.rows = t->rows;
-    t->info.n_head = t->n_head;
-    t->info.n_nodes = t->n_nodes;
-    // largest set and sum of squared set sizes
-    uint32_t mx = 0;
-    t->sum_sq_deg = 0;
-    if (t->n_head) {
-      DevBuf<unsigned long long> red(2, s);
-      EH_CUDA(cudaMemsetAsync(red.p, 0, 16, s));
-      set_size_stats_kernel<<<grid, 256, 0, s>>>(t->off.p, t->n_head, red.p);
-      EH_CHECK_LAUNCH();
-      unsigned long long h[2];
-      EH_CUDA(cudaMemcpyAsync(h, red.p, 16, cudaMemcpyDeviceToHost, s));
-      EH_CUDA(cudaStreamSynchronize(s));
-      mx = (uint32_t)h[0];
-      t->sum_sq_deg = h[1];
-    }
-    t->info.max_set = mx;
+    build_head_index(ctx, t);
+    build_stats(ctx, t);
   }
   TracePhase ph("build.reverse", s);
   trie_build_reverse(ctx, t);
@@ -694,6 +705,10 @@ __global__ void rev_fill_kernel(TrieView t, const uint32_t* __restrict__ seg, in
   }
 }
 
+static void reverse_from_keys(eh_context* ctx, eh_trie* t, DevBuf<uint32_t>& seg, DevBuf<uint32_t>& keys,
+                              DevBuf<uint32_t>& ktmp, DevBuf<uint32_t>& rowid, DevBuf<uint32_t>& vtmp,
+                              DevBuf<uint32_t>& per);
+
 void trie_build_reverse(eh_context* ctx, eh_trie* t) {
   cudaStream_t s = ctx->stream;
   const int grid = num_sms() * 8;
@@ -748,6 +763,18 @@ void trie_build_reverse(eh_context* ctx, eh_trie* t) {
   rev_key_kernel<<<grid, 256, 0, s>>>(t->view(), seg.p, t->dir, sentinel, keys.p, rowid.p, per.p);
   EH_CHECK_LAUNCH();
   ph_key.end();
+  reverse_from_keys(ctx, t, seg, keys, ktmp, rowid, vtmp, per);
+}
+
+// The reverse level from its keys (head position of b per row, sentinel for
+// rows no plan reads), the row ids and the per-b row counts: a stable sort of
+// the row ids by key, offsets, and the per-entry ranges and work.
+static void reverse_from_keys(eh_context* ctx, eh_trie* t, DevBuf<uint32_t>& seg, DevBuf<uint32_t>& keys,
+                              DevBuf<uint32_t>& ktmp, DevBuf<uint32_t>& rowid, DevBuf<uint32_t>& vtmp,
+                              DevBuf<uint32_t>& per) {
+  cudaStream_t s = ctx->stream;
+  const int grid = num_sms() * 8;
+  const int bh = bits_for(t->n_head);
   TracePhase ph_sort("reverse.sort", s);
   const uint32_t* sorted = radix_sort_payload_u32(keys.p, ktmp.p, rowid.p, vtmp.p, t->rows, bh, s);
   // only the sorted row ids are read from here on: hand the sort's other
@@ -786,6 +813,146 @@ void trie_build_reverse(eh_context* ctx, eh_trie* t) {
     EH_CUDA(cudaMemcpyAsync(&t->rev_pairs, t->rev_wpre.p + n, 8, cudaMemcpyDeviceToHost, s));
   }
   EH_CUDA(cudaStreamSynchronize(s));
+}
+
+// Rows [r0, r1) of a CSR whose values have just arrived from the host: the
+// largest value, the direction counts (rows not going up, not going down,
+// self-loops), and the reverse level's keys as if every row went up (the
+// common case; trie_build_from_host_csr recomputes them when it is not).
+// Values at or above n_alloc are outside the head index and match no head
+// entry.
+__global__ void host_chunk_kernel(TrieView t, uint64_t r0, uint64_t r1, const uint32_t* __restrict__ seg,
+                                  uint32_t n_alloc, uint32_t sentinel, uint32_t* __restrict__ keys,
+                                  uint32_t* __restrict__ rowid, uint32_t* __restrict__ per,
+                                  unsigned int* __restrict__ vmax, unsigned long long* __restrict__ cnt) {
+  unsigned int mx = 0;
+  unsigned long long not_up = 0, not_down = 0, loops = 0;
+  for (uint64_t e = r0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < r1;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t ha = seg[e];
+    const uint32_t a = t.head[ha], b = t.vals[e];
+    mx = max(mx, b);
+    not_up += b <= a;
+    not_down += b >= a;
+    loops += a == b;
+    const int32_t hb = b < n_alloc ? t.head_index[b] : -1;
+    const bool keep = hb >= 0 && e + 1 < t.off[ha + 1];
+    keys[e] = keep ? (uint32_t)hb : sentinel;
+    rowid[e] = (uint32_t)e;
+    if (keep) atomicAdd(&per[hb], 1u);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+  not_up = warp_sum(not_up);
+  not_down = warp_sum(not_down);
+  loops = warp_sum(loops);
+  if (lane_id() == 0) {
+    atomicMax(vmax, mx);
+    atomicAdd(&cnt[0], not_up);
+    atomicAdd(&cnt[1], not_down);
+    atomicAdd(&cnt[3], loops);
+  }
+}
+
+// A trie from a CSR in host memory (head[n_head] sorted distinct values,
+// off[n_head+1], vals[rows] sorted within each set), with the copy of vals
+// overlapped with the work that needs only the rows already arrived: vals go
+// up in chunks on the context's copy stream, and behind each chunk the
+// context stream computes the row sources, the direction counts and the
+// reverse level's keys.  When the relation turns out not to go up, or a value
+// lies outside the domain the head index was sized for, the reverse level is
+// rebuilt by the regular path; the trie is the same either way.
+void trie_build_from_host_csr(eh_context* ctx, eh_trie* t, const uint32_t* head, const uint64_t* off,
+                              const uint32_t* vals, uint32_t n_nodes_hint) {
+  cudaStream_t s = ctx->stream;
+  const int grid = num_sms() * 8;
+  TracePhase ph_all("host_csr.build", s);
+  t->head.alloc(t->n_head ? t->n_head : 1, s);
+  t->off.alloc(t->n_head + 1, s);
+  t->vals.alloc(t->rows ? t->rows : 1, s);
+  if (t->n_head) EH_CUDA(cudaMemcpyAsync(t->head.p, head, (size_t)t->n_head * 4, cudaMemcpyHostToDevice, s));
+  EH_CUDA(cudaMemcpyAsync(t->off.p, off, ((size_t)t->n_head + 1) * 8, cudaMemcpyHostToDevice, s));
+  if (!t->rows || !t->n_head) {
+    if (t->rows) EH_CUDA(cudaMemcpyAsync(t->vals.p, vals, t->rows * 4, cudaMemcpyHostToDevice, s));
+    const uint32_t mh = t->n_head ? max_u32(t->head.p, t->n_head, s) : 0;
+    const uint32_t mv = t->rows ? max_u32(t->vals.p, t->rows, s) : 0;
+    t->n_nodes = (t->n_head || t->rows) ? std::max(n_nodes_hint, std::max(mh, mv) + 1) : 0;
+    trie_build_from_csr(ctx, t);
+    return;
+  }
+  // vals in chunks on the copy stream, after the allocation on the context stream
+  if (!ctx->copy_stream) EH_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  constexpr int kChunks = 8;
+  cudaEvent_t ev[kChunks + 1] = {};
+  struct Events {
+    cudaEvent_t* e;
+    ~Events() {
+      for (int i = 0; i <= kChunks; i++)
+        if (e[i]) cudaEventDestroy(e[i]);
+    }
+  } guard{ev};
+  for (int i = 0; i <= kChunks; i++) EH_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
+  EH_CUDA(cudaEventRecord(ev[kChunks], s));
+  EH_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ev[kChunks], 0));
+  uint64_t bound[kChunks + 1];
+  for (int i = 0; i <= kChunks; i++) bound[i] = t->rows * (uint64_t)i / kChunks;
+  for (int i = 0; i < kChunks; i++) {
+    if (bound[i + 1] > bound[i])
+      EH_CUDA(cudaMemcpyAsync(t->vals.p + bound[i], vals + bound[i], (bound[i + 1] - bound[i]) * 4,
+                              cudaMemcpyHostToDevice, ctx->copy_stream));
+    EH_CUDA(cudaEventRecord(ev[i], ctx->copy_stream));
+  }
+  // the head index from the head alone (values beyond it are outside every set's head)
+  const uint32_t mh = max_u32(t->head.p, t->n_head, s);
+  const uint32_t n_alloc = std::max(n_nodes_hint, mh + 1);
+  t->n_nodes = n_alloc;
+  build_head_index(ctx, t);
+  DevBuf<uint32_t> seg(t->rows, s);
+  seg_kernel<<<grid, 256, 0, s>>>(t->off.p, t->n_head, seg.p);
+  EH_CHECK_LAUNCH();
+  const int bh = bits_for(t->n_head);
+  const uint32_t sentinel = (uint32_t)((1ull << bh) - 1);
+  DevBuf<uint32_t> keys(t->rows, s), ktmp(t->rows, s), rowid(t->rows, s), vtmp(t->rows, s);
+  DevBuf<uint32_t> per(t->n_head + 1, s);
+  DevBuf<unsigned long long> cnt(4, s);
+  DevBuf<unsigned int> vmax(1, s);
+  EH_CUDA(cudaMemsetAsync(per.p, 0, ((size_t)t->n_head + 1) * 4, s));
+  EH_CUDA(cudaMemsetAsync(cnt.p, 0, 32, s));
+  EH_CUDA(cudaMemsetAsync(vmax.p, 0, 4, s));
+  for (int i = 0; i < kChunks; i++) {
+    EH_CUDA(cudaStreamWaitEvent(s, ev[i], 0));
+    if (bound[i + 1] > bound[i]) {
+      host_chunk_kernel<<<grid, 256, 0, s>>>(t->view(), bound[i], bound[i + 1], seg.p, n_alloc, sentinel, keys.p,
+                                             rowid.p, per.p, vmax.p, cnt.p);
+      EH_CHECK_LAUNCH();
+    }
+  }
+  unsigned long long c[4];
+  unsigned int vm = 0;
+  EH_CUDA(cudaMemcpyAsync(c, cnt.p, 32, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaMemcpyAsync(&vm, vmax.p, 4, cudaMemcpyDeviceToHost, s));
+  EH_CUDA(cudaStreamSynchronize(s));
+  if (vm >= n_alloc) {  // a value beyond the hint and the head: the whole domain again
+    t->n_nodes = vm + 1;
+    build_head_index(ctx, t);
+  }
+  {
+    TracePhase ph("build.index+stats", s);
+    build_stats(ctx, t);
+  }
+  TracePhase ph("build.reverse", s);
+  if (vm < n_alloc && c[0] == 0) {  // every row goes up: the keys stand
+    t->dir = DIR_UP;
+    t->rev_off.alloc(t->n_head + 1, s);
+    reverse_from_keys(ctx, t, seg, keys, ktmp, rowid, vtmp, per);
+  } else {
+    seg.release();
+    keys.release();
+    ktmp.release();
+    rowid.release();
+    vtmp.release();
+    trie_build_reverse(ctx, t);
+  }
 }
 
 // Reference-format bytes of one set (see eh_trie_set_bytes in eh_b200.h).
