@@ -46,6 +46,10 @@ constexpr int kShortUnroll = EH_SHORT_UNROLL;  // flattened (row, element) pairs
 #define EH_WORD_UNROLL 1
 #endif
 constexpr int kWordUnroll = EH_WORD_UNROLL;  // flattened (row, word) pairs per lane per trip
+#ifndef EH_LONG_WORDS
+#define EH_LONG_WORDS 32
+#endif
+constexpr int kLongWords = EH_LONG_WORDS;  // word rows with at least this many words run warp-wide
 // Defaults measured on B200 at R-MAT-22 (4 KB of staging per warp leaves
 // room for 32 resident warps; 32K-probe items amortise staging); the
 // autotuner (emptyheaded_b200/autotune.py) re-picks them per trie.
@@ -408,11 +412,63 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
           abase = aa.off - aa.start;  // word w of N(a) is bs_words[abase + w]
         }
       }
-      // the word rows of this batch, flattened into (row, word) pairs over
-      // the lanes like the short element rows below: one trip covers the
-      // words of many rows
-      const uint32_t nw = (word_row && whi >= wlo) ? whi - wlo + 1 : 0u;
+      uint32_t nw = (word_row && whi >= wlo) ? whi - wlo + 1 : 0u;
       if (word_row) len = 0;  // handled here, not in the element loop
+      // long word rows (at least a warp's width of words): one row at a time
+      // across the warp, each lane ANDing words lane, lane + 32, ... with two
+      // independent loads in flight, no owner search
+      {
+        const bool is_long = nw >= (uint32_t)kLongWords;
+        uint32_t rows = __ballot_sync(kFull, is_long);
+        if (is_long) nw = 0;
+        while (rows) {
+          const int j = __ffs(rows) - 1;
+          rows &= rows - 1;
+          const uint32_t lo_w = __shfl_sync(kFull, wlo, j), hi_w = __shfl_sync(kFull, whi, j);
+          const uint32_t b0 = __shfl_sync(kFull, v0, j), b1 = __shfl_sync(kFull, v1, j);
+          const uint64_t base = __shfl_sync(kFull, abase, j);
+          const uint32_t sj = (kMode != MODE_COUNT) ? __shfl_sync(kFull, src, j) : 0u;
+          const uint32_t w_first = b0 >> 6, w_last = b1 >> 6;
+          uint32_t row_hits = 0;
+          for (uint32_t w = lo_w + lane; w <= hi_w; w += 64) {
+            const uint32_t w2 = w + 32;
+            const uint64_t a1 = __ldg(t.bs_words + base + w);
+            const uint64_t a2 = w2 <= hi_w ? __ldg(t.bs_words + base + w2) : 0ull;
+            uint64_t m1 = ~0ull, m2 = ~0ull;
+            if (w == w_first) m1 &= ~0ull << (b0 & 63);
+            if (w == w_last) m1 &= ~0ull >> (63 - (b1 & 63));
+            if (w2 == w_first) m2 &= ~0ull << (b0 & 63);
+            if (w2 == w_last) m2 &= ~0ull >> (63 - (b1 & 63));
+            const uint64_t s1 = (P == P_SBITS) ? st.words[w - st.start] : __ldg(st.words + (w - st.start));
+            const uint64_t s2 =
+                w2 <= hi_w ? ((P == P_SBITS) ? st.words[w2 - st.start] : __ldg(st.words + (w2 - st.start))) : 0ull;
+            const uint64_t x1 = a1 & s1 & m1, x2 = a2 & s2 & m2;
+            row_hits += __popcll(x1) + __popcll(x2);
+            if (kMode == MODE_MAT || (kMode == MODE_ANNOT && r.dir == DIR_SYM)) {
+              uint64_t y = x1;
+              while (y) {
+                const uint32_t bit = __ffsll((long long)y) - 1;
+                on_hit<kMode, true>(t, r, sk, sj, (w << 6) | bit);
+                y &= y - 1;
+              }
+              y = x2;
+              while (y) {
+                const uint32_t bit = __ffsll((long long)y) - 1;
+                on_hit<kMode, true>(t, r, sk, sj, (w2 << 6) | bit);
+                y &= y - 1;
+              }
+            }
+          }
+          cnt += row_hits;
+          if (kMode == MODE_ANNOT) {  // the row's source once per row
+            const uint32_t rh = warp_sum(row_hits);
+            if (lane == 0) add_src<kMode>(r, sk, sj, rh);
+          }
+        }
+      }
+      // the other word rows of this batch, flattened into (row, word) pairs
+      // over the lanes like the short element rows below: one trip covers
+      // the words of many rows
       const uint32_t wincl = warp_incl_scan(nw);
       const uint32_t wtotal = __shfl_sync(kFull, wincl, 31);
       const uint32_t wexcl = wincl - nw;
