@@ -236,6 +236,32 @@ def test_host_csr_entry(eh, oracle, golden):
     assert r == golden["synthetic"]["rmat_s12_ef16_s3"]["triangle"]
 
 
+@pytest.mark.parametrize("kind", ["up", "symmetric", "general", "hint_too_small", "big_up"])
+def test_host_csr_overlapped_build(eh, oracle, facebook, golden, kind):
+    """The host-buffer entry copies the values in chunks while it computes the
+    reverse level's keys as if every row went up; relations that do not go up,
+    and values beyond the caller's value-domain hint, take the regular build.
+    Every count must equal the oracle's."""
+    if kind == "symmetric":
+        a = facebook["duplicated"]
+        s, d = a[:, 0], a[:, 1]
+    elif kind == "general":
+        rng = np.random.default_rng(5)
+        s = rng.integers(0, 400, 8000).astype(np.uint32)
+        d = rng.integers(0, 400, 8000).astype(np.uint32)
+    elif kind == "big_up":
+        u, v = oracle.gen_rmat(42, 18, 16 << 18)
+        s, d, _ = oracle.preprocess(u, v)
+    else:
+        u, v = oracle.gen_rmat(3, 12, 16 << 12)
+        s, d, _ = oracle.preprocess(u, v)
+    o = oracle.Trie(s, d)
+    hint = 1 if kind == "hint_too_small" else int(max(s.max(), d.max())) + 1
+    for q in ("triangle", "clique4", "lollipop"):
+        got = eh.count_host_csr(o.head, o.off, o.vals, hint, query=q)
+        assert got == getattr(o, q)(), (kind, q)
+
+
 def test_autotune_keeps_counts(eh, oracle):
     from emptyheaded_b200 import autotune
     u, v = oracle.gen_rmat(42, 16, 16 << 16)
