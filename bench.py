@@ -309,7 +309,7 @@ def other_workloads(E, ctx, args, flush, deadline, model22):
             t = W.build_rmat_trie(E, 20, SEED, ctx=ctx)
             cfg = dict(AT.DEFAULT)
             qh, kh, _, _ = timed_counts(t, "clique4", cfg, steps, 2, want, flush)
-            m4, info4, prof4 = learn.train_from_trie(E, t, passes=1, epochs=40, query="clique4")
+            m4, info4, prof4 = learn.train_from_trie(E, t, passes=1, epochs=40, query="clique4", config=cfg)
             t.relayout(policy=E.LEARNED, model=m4)
             ql, kl, _, _ = timed_counts(t, "clique4", cfg, steps, 2, want, flush)
             t.relayout(policy=E.EXPLICIT, layouts=learn.best_layouts(prof4))
@@ -342,7 +342,7 @@ def other_workloads(E, ctx, args, flush, deadline, model22):
             res = {}
             for q in ("lollipop", "barbell"):
                 res[q] = timed_counts(t, q, cfg, 3, 1, int(g23[q]), flush)[0]
-            mc, infoc, _ = learn.train_from_trie(E, t, passes=1, epochs=40, query="lollipop")
+            mc, infoc, _ = learn.train_from_trie(E, t, passes=1, epochs=40, query="lollipop", config=cfg)
             t.relayout(policy=E.LEARNED, model=mc)
             for q in ("lollipop", "barbell"):
                 ql = timed_counts(t, q, cfg, 3, 1, int(g23[q]), flush)[0]
@@ -459,12 +459,12 @@ def ours_arm(args):
             torch.distributed.broadcast(p, 0)
             model.set_params(p.cpu().numpy())
         else:
-            prof = learn.profile(E, trie, reps=2)
+            prof = learn.profile(E, trie, reps=2, config=cfg_h)
             model, learn_info, _ = learn.train_from_trie(E, trie, prof=prof)
             learn_info["evaluated_on"] = "the R-MAT-22 profile it was trained on (in sample)"
             # a model trained on another graph (R-MAT-20), judged on this one
             t20 = W.build_rmat_trie(E, 20, SEED, ctx=ctx)
-            model_ho, info20, _ = learn.train_from_trie(E, t20, passes=2)
+            model_ho, info20, _ = learn.train_from_trie(E, t20, passes=2, config=cfg_h)
             t20.free()
             ho = learn.evaluate(E, model_ho, prof)
             ho["trained_on"] = "R-MAT-20 seed 42 triangle logs; evaluated on the R-MAT-22 profile (held out)"
@@ -602,24 +602,25 @@ def case_arm(args):
     t = W.build_rmat_trie(E, args.scale, SEED)
     forced = {"uint": E.UINTEGER, "bitset": E.RANGE_BITSET, "block": E.BLOCK_BITSET}
     learn_info = None
+    cfg = {k: v for k, v in (("smem_words", args.smem_words), ("warps", args.warps), ("chunk", args.chunk)) if v}
+    cfg["block_items"] = not args.no_block_items
     if args.layout == "learned":
-        model, learn_info, _ = learn.train_from_trie(E, t)
+        model, learn_info, _ = learn.train_from_trie(E, t, config=cfg)
         t.relayout(policy=E.LEARNED, model=model)
     elif args.layout in forced:
         t.relayout(policy=E.FORCED, forced=forced[args.layout], max_bitset_bytes=1 << 50)
     runs = []
-    bi = not args.no_block_items
-    t.count(args.query, block_items=bi)  # warm
+    t.count(args.query, config=cfg)  # warm
     torch.cuda.nvtx.range_push("case")
     for _ in range(args.repeat):
-        c, st = t.count(args.query, stats=True, block_items=bi)
+        c, st = t.count(args.query, stats=True, config=cfg)
         runs.append({"count": c, "query_ms": st["query_ms"], "kernel_ms": st["kernel_ms"], "wedges": st["wedges"],
                      "algorithmic_bytes": st["algorithmic_bytes"]})
     torch.cuda.nvtx.range_pop()
     g = W.golden_counts().get("rmat_s%d_ef16_s%d" % (args.scale, SEED), {})
     ok = all(r["count"] == g[args.query] for r in runs) if args.query in g else None
     print(json.dumps({"case": "rmat%d" % args.scale, "query": args.query, "layout": args.layout, "ok": ok,
-                      "block_items": bi,
+                      "schedule": cfg,
                       "info": t.info(), "learned": learn_info, "runs": runs}))
     t.free()
     return 0 if ok in (None, True) else 1
@@ -642,6 +643,9 @@ def main():
     ap.add_argument("--query", default="triangle", help="--case: query")
     ap.add_argument("--repeat", type=int, default=2, help="--case: runs inside the NVTX range")
     ap.add_argument("--no-block-items", action="store_true", help="--case: stage every N(b) per warp")
+    ap.add_argument("--smem-words", type=int, default=0, help="--case: staging words per warp")
+    ap.add_argument("--warps", type=int, default=0, help="--case: warps per block")
+    ap.add_argument("--chunk", type=int, default=0, help="--case: probes per work item")
     args = ap.parse_args()
     if args.case:
         return case_arm(args)

@@ -46,7 +46,7 @@ class EHError(RuntimeError):
 
 class LayoutConfig(ctypes.Structure):
     _fields_ = [("policy", ctypes.c_int), ("forced_layout", ctypes.c_int), ("model", ctypes.c_void_p),
-                ("max_bitset_bytes", ctypes.c_uint64), ("layouts", ctypes.c_void_p)]
+                ("max_bitset_bytes", ctypes.c_uint64), ("layouts", ctypes.c_void_p), ("min_gain", ctypes.c_float)]
 
 
 class TrieInfo(ctypes.Structure):

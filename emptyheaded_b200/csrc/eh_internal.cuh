@@ -185,6 +185,6 @@ void encoding_free(eh_encoding* e);
 
 // learned layout policy (eh_model.cu)
 void model_choose_layouts(eh_context* ctx, const eh_model* m, const eh_trie* t, uint64_t max_bitset_bytes,
-                          uint8_t* layout_dev, float* pred_dev);
+                          float min_gain, uint8_t* layout_dev, float* pred_dev);
 
 }  // namespace eh

@@ -173,8 +173,8 @@ __device__ __forceinline__ void model_features(const TrieView& t, uint32_t b, ui
 // 48x the set's uint bytes in the worst case.
 __global__ void choose_kernel(TrieView t, const uint64_t* __restrict__ rev_off, const uint64_t* __restrict__ wpre,
                               const float* __restrict__ params, const int* __restrict__ dims, int L,
-                              const int* __restrict__ woff, uint64_t max_words_per_set, uint8_t* __restrict__ layout,
-                              float* __restrict__ pred) {
+                              const int* __restrict__ woff, uint64_t max_words_per_set, float log_keep,
+                              uint8_t* __restrict__ layout, float* __restrict__ pred) {
   float buf0[64], buf1[64];
   for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.n_head; b += gridDim.x * blockDim.x) {
     const uint64_t s0 = t.off[b];
@@ -185,7 +185,9 @@ __global__ void choose_kernel(TrieView t, const uint64_t* __restrict__ rev_off, 
     if (!pairs) continue;  // never staged: keep the fallback layout
     const uint32_t words = (t.vals[s0 + len - 1] >> 6) - (t.vals[s0] >> 6) + 1;
     float best = 3.4e38f;
-    int best_l = layout[b];
+    const int h = layout[b];  // the density rule's layout: the fallback
+    int best_l = h;
+    float yh = 3.4e38f;
     const int cands[3] = {EH_LAYOUT_UINTEGER, EH_LAYOUT_RANGE_BITSET, EH_LAYOUT_BLOCK_BITSET};
     for (int c = 0; c < 3; c++) {
       const int l = cands[c];
@@ -208,10 +210,15 @@ __global__ void choose_kernel(TrieView t, const uint64_t* __restrict__ rev_off, 
         in = out;
         out = tmp;
       }
+      if (l == h) yh = in[0];
       if (in[0] < best) {
         best = in[0];
         best_l = l;
       }
+    }
+    if (best_l != h && !(best < yh + log_keep)) {  // leave the rule only for a predicted gain of min_gain
+      best_l = h;
+      best = yh;
     }
     layout[b] = (uint8_t)best_l;
     if (pred) pred[b] = fmaxf(expm1f(best), 1.f);  // the model predicts log1p(cycles)
@@ -260,8 +267,8 @@ __device__ __forceinline__ float mlp_fixed(const float* __restrict__ P, float f0
 __global__ void __launch_bounds__(128) choose_fixed_kernel(TrieView t, const uint64_t* __restrict__ rev_off,
                                                            const uint64_t* __restrict__ wpre,
                                                            const float* __restrict__ params,
-                                                           uint64_t max_words_per_set, uint8_t* __restrict__ layout,
-                                                           float* __restrict__ pred) {
+                                                           uint64_t max_words_per_set, float log_keep,
+                                                           uint8_t* __restrict__ layout, float* __restrict__ pred) {
   __shared__ float P[kFixedParams];
   for (int i = threadIdx.x; i < kFixedParams; i += blockDim.x) P[i] = params[i];
   __syncthreads();
@@ -278,21 +285,26 @@ __global__ void __launch_bounds__(128) choose_fixed_kernel(TrieView t, const uin
     // the features of model_features; the layout one-hot varies per candidate
     const float f0 = log1pf((float)len), f1 = log1pf((float)range), f2 = (float)len / ((float)range + 1.f),
                 f3 = log1pf((float)pairs);
-    float best = mlp_fixed(P, f0, f1, f2, f3, 0.f, 0.f);  // uint
+    const int h = layout[b];  // the density rule's layout: the fallback
+    const float yu = mlp_fixed(P, f0, f1, f2, f3, 0.f, 0.f);  // uint
+    const bool bits_ok = !((uint64_t)words > 16ull * len + 64 || (max_words_per_set && words > max_words_per_set));
+    const float yb = bits_ok ? mlp_fixed(P, f0, f1, f2, f3, 1.f, 0.f) : 3.4e38f;  // range bitset
+    const float yk = mlp_fixed(P, f0, f1, f2, f3, 0.f, 1.f);                      // block bitset
+    float best = yu;
     int best_l = EH_LAYOUT_UINTEGER;
-    if (!((uint64_t)words > 16ull * len + 64 || (max_words_per_set && words > max_words_per_set))) {
-      const float y = mlp_fixed(P, f0, f1, f2, f3, 1.f, 0.f);  // range bitset
-      if (y < best) {
-        best = y;
-        best_l = EH_LAYOUT_RANGE_BITSET;
-      }
+    if (yb < best) {
+      best = yb;
+      best_l = EH_LAYOUT_RANGE_BITSET;
     }
-    {
-      const float y = mlp_fixed(P, f0, f1, f2, f3, 0.f, 1.f);  // block bitset
-      if (y < best) {
-        best = y;
-        best_l = EH_LAYOUT_BLOCK_BITSET;
-      }
+    if (yk < best) {
+      best = yk;
+      best_l = EH_LAYOUT_BLOCK_BITSET;
+    }
+    // leave the rule's layout only for a predicted gain of at least min_gain
+    const float yh = h == EH_LAYOUT_RANGE_BITSET ? yb : (h == EH_LAYOUT_BLOCK_BITSET ? yk : yu);
+    if (best_l != h && !(best < yh + log_keep)) {
+      best_l = h;
+      best = yh;
     }
     layout[b] = (uint8_t)best_l;
     if (pred) pred[b] = fmaxf(expm1f(best), 1.f);  // the model predicts log1p(cycles)
@@ -300,15 +312,18 @@ __global__ void __launch_bounds__(128) choose_fixed_kernel(TrieView t, const uin
 }
 
 void model_choose_layouts(eh_context* ctx, const eh_model* m, const eh_trie* t, uint64_t max_bitset_bytes,
-                          uint8_t* layout_dev, float* pred_dev) {
+                          float min_gain, uint8_t* layout_dev, float* pred_dev) {
   cudaStream_t s = ctx->stream;
+  // the model predicts log1p(cycles): a gain g is a difference of log(1 - g)
+  const float g = min_gain == 0.f ? 0.1f : std::min(std::max(min_gain, 0.f), 0.99f);
+  const float log_keep = logf(1.f - g);
   EH_REQUIRE(m->dims[0] == kFeat && m->dims[m->n_layers] == 1, EH_ERR_INVALID,
              "layout model must map 6 features to 1 output");
   EH_REQUIRE(m->max_dim <= 64, EH_ERR_INVALID, "layout model layers must be at most 64 wide");
   if (!t->n_head || !t->rev_entries) return;
   if (m->n_layers == 3 && m->dims[1] == kH && m->dims[2] == kH && (int)m->n_params == kFixedParams) {
     choose_fixed_kernel<<<num_sms() * 4, 128, 0, s>>>(t->view(), t->rev_off.p, t->rev_wpre.p, m->params.p,
-                                                      max_bitset_bytes / 12, layout_dev, pred_dev);
+                                                      max_bitset_bytes / 12, log_keep, layout_dev, pred_dev);
     EH_CHECK_LAUNCH();
     EH_CUDA(cudaStreamSynchronize(s));
     return;
@@ -319,7 +334,8 @@ void model_choose_layouts(eh_context* ctx, const eh_model* m, const eh_trie* t, 
   EH_CUDA(cudaMemcpyAsync(ddims.p, m->dims.data(), (m->n_layers + 1) * 4, cudaMemcpyHostToDevice, s));
   EH_CUDA(cudaMemcpyAsync(dwoff.p, woff.data(), m->n_layers * 4, cudaMemcpyHostToDevice, s));
   choose_kernel<<<num_sms() * 2, 128, 0, s>>>(t->view(), t->rev_off.p, t->rev_wpre.p, m->params.p, ddims.p,
-                                               m->n_layers, dwoff.p, max_bitset_bytes / 12, layout_dev, pred_dev);
+                                               m->n_layers, dwoff.p, max_bitset_bytes / 12, log_keep, layout_dev,
+                                               pred_dev);
   EH_CHECK_LAUNCH();
   EH_CUDA(cudaStreamSynchronize(s));
 }

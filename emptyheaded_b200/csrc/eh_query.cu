@@ -147,6 +147,15 @@ __device__ __forceinline__ uint32_t staged_words(const TrieView& t, uint32_t b) 
   return 0xffffffffu;  // block bitsets are probed in global memory
 }
 
+// A block item keeps every warp of the block on one staged N(b); a b with
+// little work would leave most of them idle, so only a b with at least this
+// many probes becomes block items (about 32 batches of 32 rows at R-MAT's
+// row lengths); the others stay warp items probing N(b) in global memory.
+#ifndef EH_MIN_BLOCK_WORK
+#define EH_MIN_BLOCK_WORK (1ull << 17)
+#endif
+constexpr uint64_t kMinBlockWork = EH_MIN_BLOCK_WORK;
+
 struct PlanShape {
   uint32_t chunk;        // probes per warp item
   const float* pred;     // predicted cycles of each head entry's work (learned layouts), or null
@@ -161,7 +170,7 @@ __global__ void plan_split_kernel(TrieView t, RevView r, PlanShape ps, uint32_t*
   for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.n_head; b += gridDim.x * blockDim.x) {
     const uint64_t w = r.rev_wpre[r.rev_off[b + 1]] - r.rev_wpre[r.rev_off[b]];
     const uint32_t sw = staged_words(t, b);
-    const bool blk = ps.block_words && sw > ps.warp_words && sw <= ps.block_words;
+    const bool blk = ps.block_words && sw > ps.warp_words && sw <= ps.block_words && w >= kMinBlockWork;
     const uint64_t mult = blk ? ps.warps : 1;
     uint64_t n = 0;
     if (w) {

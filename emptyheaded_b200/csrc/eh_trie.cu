@@ -495,7 +495,7 @@ void trie_layout(eh_context* ctx, eh_trie* t, const eh_layout_config* cfg) {
   if (policy == EH_POLICY_LEARNED) {
     EH_REQUIRE(cfg->model != nullptr, EH_ERR_INVALID, "learned layout policy needs a model");
     if (t->n_head && t->rev_pairs) t->work_pred.alloc(t->n_head, s);
-    model_choose_layouts(ctx, cfg->model, t, cfg->max_bitset_bytes, t->layout.p, t->work_pred.p);
+    model_choose_layouts(ctx, cfg->model, t, cfg->max_bitset_bytes, cfg->min_gain, t->layout.p, t->work_pred.p);
     if (t->work_pred.p) {
       DevBuf<double> sum(1, s);
       EH_CUDA(cudaMemsetAsync(sum.p, 0, 8, s));

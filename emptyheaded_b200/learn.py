@@ -38,12 +38,14 @@ def set_features(head_len, rng, pairs, layout):
     return f
 
 
-def profile(E, trie, reps=2, query="triangle"):
+def profile(E, trie, reps=2, query="triangle", config=None):
     """Per-set cycles of `query`'s intersection kernel under each layout
     (the triangle or 4-clique kernel; for lollipop / barbell, the annotated
     triangle pass that dominates them).  Returns (len, range, pairs,
     cycles[layout] with NaN where the layout was not admissible, base
-    heuristic layout)."""
+    heuristic layout).  `config` is the schedule (autotune dict) the timed
+    runs will use: costs depend on it (the staging capacity per warp above
+    all), so the profile runs with the same one."""
     head, off, vals, heur = trie.export()
     n = len(head)
     lens = np.diff(off).astype(np.float64)
@@ -65,7 +67,7 @@ def profile(E, trie, reps=2, query="triangle"):
         _, _, _, lay = trie.export()
         acc = np.zeros(n)
         for _ in range(reps):
-            trie.count(query, record=True)
+            trie.count(query, record=True, config=config)
             rec = E.timing_records(trie.ctx)
             hb = rec[:, 6].view(np.uint32).astype(np.int64)
             acc += np.bincount(hb, weights=rec[:, 7].astype(np.float64), minlength=n)
@@ -77,14 +79,23 @@ def profile(E, trie, reps=2, query="triangle"):
     return dict(lens=lens, range=rng, pairs=pairs, cycles=cycles, heuristic=heur.astype(np.int64), words=words)
 
 
-def dataset(prof):
+def dataset(prof, max_weight=32):
+    """Training rows (features, log1p cycles), one per staged set and
+    admissible layout.  A set's row is repeated in proportion to its cost
+    (at most max_weight times): the sets that hold the time are the ones the
+    choice has to get right, and most sets are cheap."""
     xs, ys = [], []
     staged = prof["pairs"] > 0
     for L in LAYOUTS:
         c = prof["cycles"][L]
         m = staged & np.isfinite(c) & (c > 0)
-        xs.append(set_features(prof["lens"][m], prof["range"][m], prof["pairs"][m], np.full(m.sum(), L)))
-        ys.append(np.log1p(c[m]).astype(np.float32)[:, None])
+        if not m.any():
+            continue
+        reps = np.clip(np.round(c[m] / c[m].mean()), 1, max_weight).astype(np.int64)
+        f = set_features(prof["lens"][m], prof["range"][m], prof["pairs"][m], np.full(m.sum(), L))
+        y = np.log1p(c[m]).astype(np.float32)[:, None]
+        xs.append(np.repeat(f, reps, axis=0))
+        ys.append(np.repeat(y, reps, axis=0))
     return np.concatenate(xs), np.concatenate(ys)
 
 
@@ -177,10 +188,10 @@ def best_layouts(prof):
     return np.where(staged, pick, prof["heuristic"].astype(np.uint8)).astype(np.uint8)
 
 
-def train_from_trie(E, trie, passes=2, epochs=60, query="triangle", prof=None):
+def train_from_trie(E, trie, passes=2, epochs=60, query="triangle", prof=None, config=None):
     """Profile `trie` (or take its profile), train the cost model on the
     logs, evaluate it on the same logs.  Returns (model, info, profile)."""
-    prof = prof if prof is not None else profile(E, trie, reps=passes, query=query)
+    prof = prof if prof is not None else profile(E, trie, reps=passes, query=query, config=config)
     x, y = dataset(prof)
     model, losses = train(E, x, y, ctx=trie.ctx, epochs=epochs)
     info = evaluate(E, model, prof)

@@ -149,6 +149,10 @@ typedef struct {
    * per-element bound. */
   uint64_t max_bitset_bytes;
   const uint8_t* layouts; /* EH_POLICY_EXPLICIT: host array, one EH_LAYOUT_* per level-1 set (n_head) */
+  /* LEARNED: a set leaves the density rule's layout only when the model
+   * predicts at least this fraction less cost for another (0: 0.1), so
+   * that small prediction errors do not move sets for nothing. */
+  float min_gain;
 } eh_layout_config;
 
 typedef struct {
