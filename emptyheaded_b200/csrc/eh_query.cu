@@ -1063,6 +1063,17 @@ static int blocks_per_sm(const void* kernel, int threads, size_t smem) {
   return std::max(1, b);
 }
 
+// dynamic shared memory a block of `kernel` may use: the device's opt-in
+// per-block limit less the kernel's own static shared memory
+static size_t dynamic_smem_room(const void* kernel) {
+  int dev = 0, optin = 0;
+  EH_CUDA(cudaGetDevice(&dev));
+  EH_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  EH_CUDA(cudaFuncGetAttributes(&fa, kernel));
+  return (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+}
+
 template <typename K>
 static void set_smem_attr(K kernel, size_t smem) {
   EH_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1140,15 +1151,20 @@ static void prepare(eh_context* ctx, const eh_trie* const* tries, uint32_t n, in
   if (annot && !ep.smem_given) ep.smem_words = 2 * kDefaultSmemWords;
   P.threads = 32 * ep.warps;
   P.smem = (size_t)ep.smem_words * 4 * ep.warps;
+  const void* kfn;
+  if (query == EH_QUERY_CLIQUE4) kfn = (const void*)clique4_kernel;
+  else if (annot) kfn = (const void*)triangle_kernel<MODE_ANNOT>;
+  else kfn = (const void*)triangle_kernel<MODE_COUNT>;
   {
-    int dev = 0, optin = 0;
-    EH_CUDA(cudaGetDevice(&dev));
-    EH_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    if (P.smem > (size_t)optin) {
+    size_t room = dynamic_smem_room(kfn);
+    // the materializing pass launches MODE_MAT with the same shape
+    if (!annot && query != EH_QUERY_CLIQUE4)
+      room = std::min(room, dynamic_smem_room((const void*)triangle_kernel<MODE_MAT>));
+    if (P.smem > room) {
       // shrink the per-warp region to what a block may hold (a staged set
       // that no longer fits is probed in global memory instead)
       EH_REQUIRE(query != EH_QUERY_CLIQUE4, EH_ERR_UNSUPPORTED, "4-clique staging exceeds shared memory");
-      ep.smem_words = (int)((optin / 4 / ep.warps) & ~1);
+      ep.smem_words = (int)((room / 4 / ep.warps) & ~(size_t)1);
       P.smem = (size_t)ep.smem_words * 4 * ep.warps;
     }
   }
@@ -1196,17 +1212,9 @@ static void prepare(eh_context* ctx, const eh_trie* const* tries, uint32_t n, in
   P.q.alloc(2, s);
   EH_CUDA(cudaMemcpyAsync(P.dv.p, hv.data(), n * sizeof(TrieView), cudaMemcpyHostToDevice, s));
   EH_CUDA(cudaMemcpyAsync(P.dr.p, hr.data(), n * sizeof(RevView), cudaMemcpyHostToDevice, s));
-  const void* kfn;
-  if (query == EH_QUERY_CLIQUE4) {
-    set_smem_attr(clique4_kernel, P.smem);
-    kfn = (const void*)clique4_kernel;
-  } else if (annot) {
-    set_smem_attr(triangle_kernel<MODE_ANNOT>, P.smem);
-    kfn = (const void*)triangle_kernel<MODE_ANNOT>;
-  } else {
-    set_smem_attr(triangle_kernel<MODE_COUNT>, P.smem);
-    kfn = (const void*)triangle_kernel<MODE_COUNT>;
-  }
+  if (query == EH_QUERY_CLIQUE4) set_smem_attr(clique4_kernel, P.smem);
+  else if (annot) set_smem_attr(triangle_kernel<MODE_ANNOT>, P.smem);
+  else set_smem_attr(triangle_kernel<MODE_COUNT>, P.smem);
   const int per_sm = blocks_per_sm(kfn, P.threads, P.smem);
   const uint64_t units = (uint64_t)total_b + (total_items - total_b + ep.warps - 1) / ep.warps;
   P.grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms() * per_sm, units));
@@ -1802,15 +1810,13 @@ void query_count_in_scratch(eh_context* ctx, const eh_trie* t, int query, const 
   // launch shape and shared memory, checked before anything is launched
   const int threads = 32 * ep.warps;
   const size_t smem = (size_t)ep.smem_words * 4 * ep.warps;
-  {
-    int dev = 0, optin = 0;
-    EH_CUDA(cudaGetDevice(&dev));
-    EH_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    EH_REQUIRE(smem <= (size_t)optin, EH_ERR_UNSUPPORTED,
-               "shared staging of " + std::to_string(smem) + " bytes per block is above the device's limit of " +
-                   std::to_string(optin));
-  }
   const void* kfn = clique ? (const void*)clique4_kernel : (const void*)triangle_kernel<MODE_COUNT>;
+  {
+    const size_t room = dynamic_smem_room(kfn);
+    EH_REQUIRE(smem <= room, EH_ERR_UNSUPPORTED,
+               "shared staging of " + std::to_string(smem) + " bytes per block is above the " + std::to_string(room) +
+                   " a block may use");
+  }
   if (clique) set_smem_attr(clique4_kernel, smem);
   else set_smem_attr(triangle_kernel<MODE_COUNT>, smem);
   const int per_sm = blocks_per_sm(kfn, threads, smem);
