@@ -135,14 +135,27 @@ __global__ void plan_fill_kernel(RevView r, uint32_t nh, const uint32_t* __restr
   }
 }
 
+// u32 words a compressed staging (P_ZBITS, below) of a W-word range bitset
+// with len elements takes at most: W/32 presence words, as many ranks, and
+// at most min(len, W) non-zero 64-bit words, at an even offset
+__host__ __device__ __forceinline__ uint32_t zbits_words(uint32_t W, uint32_t len) {
+  const uint32_t groups = (W + 31) / 32;
+  return ((2 * groups + 1) & ~1u) + 2 * (len < W ? len : W);
+}
+
 // Work of head entry b is staged in one of two classes: per warp (N(b)
 // fits a warp's shared region, or must be probed in global memory) or per
 // block (N(b) needs more than a warp's region but fits the block's: every
 // warp of the block works on the rows of one staged N(b)).  A block item
 // holds `warps` times a warp item's work.
-__device__ __forceinline__ uint32_t staged_words(const TrieView& t, uint32_t b) {
+__device__ __forceinline__ uint32_t staged_words(const TrieView& t, uint32_t b, uint32_t warp_words) {
   const uint8_t l = t.layout[b];
-  if (l == EH_LAYOUT_RANGE_BITSET) return 2u * t.aux[b].n;
+  if (l == EH_LAYOUT_RANGE_BITSET) {
+    const uint32_t raw = 2u * t.aux[b].n;
+    if (raw <= warp_words) return raw;
+    const uint32_t z = zbits_words(t.aux[b].n, (uint32_t)(t.off[b + 1] - t.off[b]));
+    return z <= warp_words ? z : raw;  // compressed in a warp, or raw across a block
+  }
   if (l == EH_LAYOUT_UINTEGER) return (uint32_t)(t.off[b + 1] - t.off[b]);
   return 0xffffffffu;  // block bitsets are probed in global memory
 }
@@ -169,7 +182,7 @@ __global__ void plan_split_kernel(TrieView t, RevView r, PlanShape ps, uint32_t*
                                   uint32_t* __restrict__ nb) {
   for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < t.n_head; b += gridDim.x * blockDim.x) {
     const uint64_t w = r.rev_wpre[r.rev_off[b + 1]] - r.rev_wpre[r.rev_off[b]];
-    const uint32_t sw = staged_words(t, b);
+    const uint32_t sw = staged_words(t, b, ps.warp_words);
     const bool blk = ps.block_words && sw > ps.warp_words && sw <= ps.block_words && w >= kMinBlockWork;
     const uint64_t mult = blk ? ps.warps : 1;
     uint64_t n = 0;
@@ -226,16 +239,23 @@ static uint32_t build_plan(eh_context* ctx, const eh_trie* t, const PlanShape& s
 
 // ------------------------------------------------------------------ probes
 // Probe structures for the staged set N(b), one per stored layout.
-enum { P_SBITS = 0, P_GBITS = 1, P_SLIST = 2, P_GLIST = 3, P_GBLOCK = 4 };
+// P_ZBITS: a range bitset too large to stage word for word, staged
+// compressed: a presence bit per 64-bit word, the count of non-zero words
+// before each group of 32 words, and only the non-zero words.  A probe that
+// misses (most of them) costs one shared load; a hit three.
+enum { P_SBITS = 0, P_GBITS = 1, P_SLIST = 2, P_GLIST = 3, P_GBLOCK = 4, P_ZBITS = 5 };
 
 struct Staged {
-  const uint64_t* words;  // P_SBITS (shared) / P_GBITS (global)
+  const uint64_t* words;  // P_SBITS (shared) / P_GBITS (global); P_ZBITS: the non-zero words (shared)
   const uint32_t* list;   // P_SLIST (shared) / P_GLIST (global)
   const uint32_t* ids;    // P_GBLOCK
   const uint64_t* bwords; // P_GBLOCK
+  const uint32_t* pres;   // P_ZBITS: presence bit of word i at bit i % 32 of pres[i / 32]
+  const uint32_t* zrank;  // P_ZBITS: non-zero words before word 32 * k
   uint32_t start;         // first word index (bitsets)
   uint32_t n;             // words / list length / blocks
 };
+
 
 // branch-free lower bound over a sorted run of n >= 1 values
 template <bool kShared>
@@ -252,6 +272,14 @@ __device__ __forceinline__ bool list_contains(const uint32_t* p, uint32_t n, uin
 
 template <int P>
 __device__ __forceinline__ uint32_t probe(const Staged& s, uint32_t w) {
+  if (P == P_ZBITS) {
+    const uint32_t idx = (w >> 6) - s.start;
+    if (idx >= s.n) return 0;  // also catches w below the first word (wraps)
+    const uint32_t p = s.pres[idx >> 5];
+    const uint32_t below = p & ((1u << (idx & 31)) - 1u);
+    if (!((p >> (idx & 31)) & 1u)) return 0;
+    return (uint32_t)(s.words[s.zrank[idx >> 5] + __popc(below)] >> (w & 63)) & 1u;
+  }
   if (P == P_SBITS || P == P_GBITS) {
     const uint32_t idx = (w >> 6) - s.start;
     if (idx >= s.n) return 0;  // also catches w below the first word (wraps)
@@ -605,6 +633,40 @@ __device__ __forceinline__ int stage_set(const TrieView& t, uint32_t hb, uint32_
       st.words = sw;
       return P_SBITS;
     }
+    if (zbits_words(a.n, len) <= (uint32_t)cap_words) {
+      // compressed: 32 words per step, 4 steps of loads in flight
+      const uint32_t groups = (a.n + 31) / 32;
+      uint32_t* pres = sm;
+      uint32_t* zr = sm + groups;
+      uint64_t* zw = reinterpret_cast<uint64_t*>(sm + ((2 * groups + 1) & ~1u));
+      const uint64_t* src = t.bs_words + a.off;
+      uint32_t run = 0;
+      for (uint32_t g0 = 0; g0 < groups; g0 += 4) {
+        uint64_t x[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const uint32_t j = (g0 + u) * 32 + lane;
+          x[u] = j < a.n ? __ldg(src + j) : 0ull;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          if (g0 + u < groups) {
+            const uint32_t bal = __ballot_sync(kFull, x[u] != 0ull);
+            if (x[u]) zw[run + __popc(bal & lanemask_lt())] = x[u];
+            if (lane == 0) {
+              pres[g0 + u] = bal;
+              zr[g0 + u] = run;
+            }
+            run += __popc(bal);
+          }
+        }
+      }
+      __syncwarp();
+      st.pres = pres;
+      st.zrank = zr;
+      st.words = zw;
+      return P_ZBITS;
+    }
     st.words = t.bs_words + a.off;
     return P_GBITS;
   }
@@ -669,6 +731,7 @@ __device__ __forceinline__ uint64_t rows_of(int mode, const Staged& st, const Tr
     case P_GBITS: return stream_rows<P_GBITS, kMode>(st, t, r, kb, ke, long_row, sk);
     case P_SLIST: return stream_rows<P_SLIST, kMode>(st, t, r, kb, ke, long_row, sk);
     case P_GLIST: return stream_rows<P_GLIST, kMode>(st, t, r, kb, ke, long_row, sk);
+    case P_ZBITS: return stream_rows<P_ZBITS, kMode>(st, t, r, kb, ke, long_row, sk);
     default: return stream_rows<P_GBLOCK, kMode>(st, t, r, kb, ke, long_row, sk);
   }
 }
@@ -975,6 +1038,7 @@ __global__ void EH_TRI_LAUNCH_BOUNDS clique4_kernel(const TrieView* __restrict__
       case P_GBITS: c = clique_rows<P_GBITS>(st, t, r, item.kb, item.ke, sbuf, scap, out.sel, wb); break;
       case P_SLIST: c = clique_rows<P_SLIST>(st, t, r, item.kb, item.ke, sbuf, scap, out.sel, wb); break;
       case P_GLIST: c = clique_rows<P_GLIST>(st, t, r, item.kb, item.ke, sbuf, scap, out.sel, wb); break;
+      case P_ZBITS: c = clique_rows<P_ZBITS>(st, t, r, item.kb, item.ke, sbuf, scap, out.sel, wb); break;
       default: c = clique_rows<P_GBLOCK>(st, t, r, item.kb, item.ke, sbuf, scap, out.sel, wb); break;
     }
     acc += warp_sum(c);

@@ -287,3 +287,27 @@ def test_context_close_frees_dependents(eh, facebook):
     assert t.h is None and m.h is None
     t.free()
     c.close()
+
+
+@pytest.mark.parametrize("smem", [64, 256, 1024])
+def test_compressed_bitset_staging(eh, oracle, smem):
+    """Range bitsets too large for a warp's region are staged compressed
+    (presence bits, ranks, non-zero words) when that fits: forcing every
+    admissible set to a bitset and shrinking the region sends most sets
+    through that path, in the COUNT, 4-clique, annotated and materializing
+    kernels.  Counts and rows must not change."""
+    u, v = oracle.gen_rmat(42, 14, 16 << 14)
+    s, d, _ = oracle.preprocess(u, v)
+    o = oracle.Trie(s, d)
+    t = eh.Trie(s, d, policy=2, forced=0, max_bitset_bytes=1 << 50)
+    cfg = {"smem_words": smem}
+    assert t.count("triangle", config=cfg) == o.triangle()
+    assert t.count("clique4", config=cfg) == o.clique4()
+    assert t.count("lollipop", config=cfg) == o.lollipop()
+    assert t.count("barbell", config=cfg) == o.barbell()
+    assert t.count("triangle", config=dict(cfg, warps=4, long_row=1)) == o.triangle()
+    t.free()
+    a = oracle.Trie(*(np.array(x, np.uint32) for x in (s, d)))
+    ts = eh.Trie(s, d, policy=2, forced=0, max_bitset_bytes=1 << 50)
+    np.testing.assert_array_equal(ts.materialize(), a.triangle_tuples())
+    ts.free()
