@@ -18,7 +18,7 @@ checked against the first one, so tuning can never change a result.
 import statistics
 
 GRID = {
-    "smem_words": (1024, 1536, 1664, 1792, 2048),
+    "smem_words": (512, 1024, 1536),
     "chunk": (16384, 32768, 65536, 131072),
     "long_row": (16, 32, 64, 128),
     "warps": (4, 8, 16),
