@@ -50,6 +50,10 @@ constexpr int kWordUnroll = EH_WORD_UNROLL;  // flattened (row, word) pairs per 
 #define EH_LONG_WORDS 32
 #endif
 constexpr int kLongWords = EH_LONG_WORDS;  // word rows with at least this many words run warp-wide
+#ifndef EH_FLAT_CLIQUE
+#define EH_FLAT_CLIQUE 48
+#endif
+constexpr uint32_t kFlatClique = EH_FLAT_CLIQUE;  // 4-clique: S up to this size has its pairs flattened
 // Defaults measured on B200 at R-MAT-22 (4 KB of staging per warp leaves
 // room for 32 resident warps; 32K-probe items amortise staging); the
 // autotuner (emptyheaded_b200/autotune.py) re-picks them per trie.
@@ -979,6 +983,37 @@ __device__ uint64_t clique_rows(const Staged& st, const TrieView& t, const RevVi
     }
     __syncwarp();
     if (ns > cap) ns = cap;  // capacity bound checked by the host planner
+    // small S: the (c, d) pairs flattened over the lanes, so a warp step
+    // probes 32 pairs whatever the length of each c's run
+    if (ns <= kFlatClique) {
+      const uint32_t np = general ? ns * ns : ns * (ns - 1) / 2;
+      for (uint32_t p = lane; p < np; p += 32) {
+        uint32_t i, j;  // the pair's positions in S: i < j unless general
+        if (general) {
+          i = p / ns;
+          j = p - i * ns;
+        } else {
+          // row i of the triangular pair index holds ns - 1 - i pairs and
+          // starts at i * ns - i * (i + 1) / 2; a float guess, then exact steps
+          const float m = (float)(2 * ns - 1);
+          int g = (int)floorf((m - sqrtf(fmaxf(m * m - 8.f * (float)p, 0.f))) * 0.5f);
+          g = max(0, min(g, (int)ns - 2));
+          i = (uint32_t)g;
+          while (i + 1 < ns - 1 && (i + 1) * ns - (i + 1) * (i + 2) / 2 <= p) i++;
+          while (i > 0 && i * ns - i * (i + 1) / 2 > p) i--;
+          j = p - (i * ns - i * (i + 1) / 2) + i + 1;
+        }
+        // up (and general): probe d = S[j] in N(S[i]); down: d = S[i] in N(S[j])
+        const uint32_t c = (up || general) ? sbuf[i] : sbuf[j];
+        const uint32_t dd = (up || general) ? sbuf[j] : sbuf[i];
+        const int32_t hc = __ldg(t.head_index + c);
+        if (hc < 0) continue;
+        if (probe_global_set(t, (uint32_t)hc, dd))
+          cnt += (sel && r.dir == DIR_SYM) ? wab + sel_bit(sel, c) + sel_bit(sel, dd) : 1u;
+      }
+      __syncwarp();
+      continue;
+    }
     // for each c = S[i]: count S elements beyond c (up) or before c (down) in N(c)
     for (uint32_t i = 0; i < ns; i++) {
       const uint32_t c = sbuf[i];
