@@ -602,7 +602,8 @@ def case_arm(args):
     t = W.build_rmat_trie(E, args.scale, SEED)
     forced = {"uint": E.UINTEGER, "bitset": E.RANGE_BITSET, "block": E.BLOCK_BITSET}
     learn_info = None
-    cfg = {k: v for k, v in (("smem_words", args.smem_words), ("warps", args.warps), ("chunk", args.chunk)) if v}
+    cfg = {k: v for k, v in (("smem_words", args.smem_words), ("warps", args.warps), ("chunk", args.chunk),
+                             ("long_row", args.long_row)) if v}
     cfg["block_items"] = not args.no_block_items
     if args.layout == "learned":
         model, learn_info, _ = learn.train_from_trie(E, t, config=cfg)
@@ -646,6 +647,7 @@ def main():
     ap.add_argument("--smem-words", type=int, default=0, help="--case: staging words per warp")
     ap.add_argument("--warps", type=int, default=0, help="--case: warps per block")
     ap.add_argument("--chunk", type=int, default=0, help="--case: probes per work item")
+    ap.add_argument("--long-row", type=int, default=0, help="--case: rows at least this long run warp-wide")
     args = ap.parse_args()
     if args.case:
         return case_arm(args)
