@@ -111,40 +111,68 @@ __global__ void plan_count_kernel(RevView r, uint32_t nh, uint32_t chunk, uint32
 }
 // item i of b covers the rows whose work prefix falls in [i, i+1) * W/n;
 // items are written in reverse head order so the queue starts at the
-// largest-degree b (ids are degree-ordered) and small items come last
+// largest-degree b (ids are degree-ordered) and small items come last.
+// first row k in [lo, hi) with wpre[k] >= target (hi if none)
+__device__ __forceinline__ uint64_t first_row_at(const uint64_t* __restrict__ wpre, uint64_t lo, uint64_t hi,
+                                                 uint64_t target) {
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (wpre[mid] < target) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// A lane cuts the items of its own head entry one after the other; an
+// entry with more than kFillSerial items (a hub b) is cut by the whole
+// warp, each lane bounding its items with two independent searches, so one
+// thread never holds the planner up for hundreds of searches.  The bounds
+// are the same either way: the work prefix is non-decreasing, so the first
+// row at target i+1 searched from k0 is the one searched from item i's end.
+constexpr uint32_t kFillSerial = 8;
 __global__ void plan_fill_kernel(RevView r, uint32_t nh, const uint32_t* __restrict__ nitems,
                                  const uint32_t* __restrict__ ipos, uint32_t total, uint32_t g,
                                  Item* __restrict__ items) {
-  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nh; b += gridDim.x * blockDim.x) {
-    const uint32_t n = nitems[b];
-    if (!n) continue;
-    const uint64_t k0 = r.rev_off[b], k1 = r.rev_off[b + 1];
-    const uint64_t w0 = r.rev_wpre[k0], W = r.rev_wpre[k1] - w0;
-    uint64_t kb = k0;
-    for (uint32_t i = 0; i < n; i++) {
-      uint64_t ke = k1;
-      if (i + 1 < n) {
-        const uint64_t target = w0 + (W * (i + 1)) / n;
-        uint64_t lo = kb, hi = k1;  // first k with wpre[k] >= target
-        while (lo < hi) {
-          const uint64_t mid = (lo + hi) >> 1;
-          if (r.rev_wpre[mid] < target) lo = mid + 1; else hi = mid;
-        }
-        ke = lo;
+  const uint32_t lane = lane_id();
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint64_t base = (uint64_t)warp * 32; base < nh; base += (uint64_t)nwarps * 32) {
+    const uint32_t b = (uint32_t)base + lane;
+    const uint32_t n = b < nh ? nitems[b] : 0u;
+    if (n && n <= kFillSerial) {
+      const uint64_t k0 = r.rev_off[b], k1 = r.rev_off[b + 1];
+      const uint64_t w0 = r.rev_wpre[k0], W = r.rev_wpre[k1] - w0;
+      uint64_t kb = k0;
+      for (uint32_t i = 0; i < n; i++) {
+        const uint64_t ke = i + 1 < n ? first_row_at(r.rev_wpre, kb, k1, w0 + (W * (i + 1)) / n) : k1;
+        items[total - 1 - (ipos[b] + i)] = Item{b, (uint32_t)kb, (uint32_t)ke, g};
+        kb = ke;
       }
-      if (ke > kb) items[total - 1 - (ipos[b] + i)] = Item{b, (uint32_t)kb, (uint32_t)ke, g};
-      else items[total - 1 - (ipos[b] + i)] = Item{b, (uint32_t)kb, (uint32_t)kb, g};
-      kb = ke;
+    }
+    uint32_t hubs = __ballot_sync(kFull, n > kFillSerial);
+    while (hubs) {
+      const int j = __ffs(hubs) - 1;
+      hubs &= hubs - 1;
+      const uint32_t bj = (uint32_t)base + j;
+      const uint32_t nj = __shfl_sync(kFull, n, j);
+      const uint64_t k0 = r.rev_off[bj], k1 = r.rev_off[bj + 1];
+      const uint64_t w0 = r.rev_wpre[k0], W = r.rev_wpre[k1] - w0;
+      const uint32_t p0 = ipos[bj];
+      for (uint32_t i = lane; i < nj; i += 32) {
+        const uint64_t kb = i ? first_row_at(r.rev_wpre, k0, k1, w0 + (W * i) / nj) : k0;
+        const uint64_t ke = i + 1 < nj ? first_row_at(r.rev_wpre, kb, k1, w0 + (W * (i + 1)) / nj) : k1;
+        items[total - 1 - (p0 + i)] = Item{bj, (uint32_t)kb, (uint32_t)ke, g};
+      }
     }
   }
 }
 
+
 // u32 words a compressed staging (P_ZBITS, below) of a W-word range bitset
-// with len elements takes at most: W/32 presence words, as many ranks, and
-// at most min(len, W) non-zero 64-bit words, at an even offset
+// with len elements takes at most: a (presence mask, rank) pair per 32 words
+// and at most min(len, W) non-zero 64-bit words
 __host__ __device__ __forceinline__ uint32_t zbits_words(uint32_t W, uint32_t len) {
   const uint32_t groups = (W + 31) / 32;
-  return ((2 * groups + 1) & ~1u) + 2 * (len < W ? len : W);
+  return 2 * groups + 2 * (len < W ? len : W);
 }
 
 // Work of head entry b is staged in one of two classes: per warp (N(b)
@@ -244,9 +272,10 @@ static uint32_t build_plan(eh_context* ctx, const eh_trie* t, const PlanShape& s
 // ------------------------------------------------------------------ probes
 // Probe structures for the staged set N(b), one per stored layout.
 // P_ZBITS: a range bitset too large to stage word for word, staged
-// compressed: a presence bit per 64-bit word, the count of non-zero words
-// before each group of 32 words, and only the non-zero words.  A probe that
-// misses (most of them) costs one shared load; a hit three.
+// compressed: per group of 32 words a presence mask (bit i: word 32k + i is
+// non-zero) beside the count of non-zero words before the group, read
+// together in one 8-byte load, and then only the non-zero words.  A probe
+// whose word is empty costs one shared load; the others two.
 enum { P_SBITS = 0, P_GBITS = 1, P_SLIST = 2, P_GLIST = 3, P_GBLOCK = 4, P_ZBITS = 5 };
 
 struct Staged {
@@ -254,8 +283,7 @@ struct Staged {
   const uint32_t* list;   // P_SLIST (shared) / P_GLIST (global)
   const uint32_t* ids;    // P_GBLOCK
   const uint64_t* bwords; // P_GBLOCK
-  const uint32_t* pres;   // P_ZBITS: presence bit of word i at bit i % 32 of pres[i / 32]
-  const uint32_t* zrank;  // P_ZBITS: non-zero words before word 32 * k
+  const uint2* pz;        // P_ZBITS: group k: x = presence mask of words 32k.., y = non-zero words before 32k
   uint32_t start;         // first word index (bitsets)
   uint32_t n;             // words / list length / blocks
 };
@@ -279,10 +307,10 @@ __device__ __forceinline__ uint32_t probe(const Staged& s, uint32_t w) {
   if (P == P_ZBITS) {
     const uint32_t idx = (w >> 6) - s.start;
     if (idx >= s.n) return 0;  // also catches w below the first word (wraps)
-    const uint32_t p = s.pres[idx >> 5];
-    const uint32_t below = p & ((1u << (idx & 31)) - 1u);
-    if (!((p >> (idx & 31)) & 1u)) return 0;
-    return (uint32_t)(s.words[s.zrank[idx >> 5] + __popc(below)] >> (w & 63)) & 1u;
+    const uint2 g = s.pz[idx >> 5];
+    if (!((g.x >> (idx & 31)) & 1u)) return 0;
+    const uint32_t below = g.x & ((1u << (idx & 31)) - 1u);
+    return (uint32_t)(s.words[g.y + __popc(below)] >> (w & 63)) & 1u;
   }
   if (P == P_SBITS || P == P_GBITS) {
     const uint32_t idx = (w >> 6) - s.start;
@@ -552,8 +580,9 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
         }
       }
     }
-    // ---- long element rows: one row at a time across the warp, two
-    // coalesced elements per lane per trip, no owner search
+    // ---- long element rows: two rows at a time across the warp, each lane
+    // loading kLongUnroll coalesced elements of both before it probes any,
+    // no owner search
     {
       const bool is_long = len >= long_row;
       uint32_t rows = __ballot_sync(kFull, is_long);
@@ -562,15 +591,32 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
       while (rows) {
         const int j = __ffs(rows) - 1;
         rows &= rows - 1;
+        int j2 = j;
+        bool two = false;
+        if (rows) {
+          j2 = __ffs(rows) - 1;
+          rows &= rows - 1;
+          two = true;
+        }
         const uint32_t rlo = __shfl_sync(kFull, lo, j), rn = __shfl_sync(kFull, rlen, j);
-        uint32_t src_j = 0;
-        if (kMode != MODE_COUNT) src_j = __shfl_sync(kFull, src, j);
+        const uint32_t rlo2 = __shfl_sync(kFull, lo, j2);
+        const uint32_t rn2 = two ? __shfl_sync(kFull, rlen, j2) : 0u;
+        uint32_t src_j = 0, src_j2 = 0;
+        if (kMode != MODE_COUNT) {
+          src_j = __shfl_sync(kFull, src, j);
+          src_j2 = __shfl_sync(kFull, src, j2);
+        }
         const uint32_t* row = t.vals + rlo;
-        uint32_t row_hits = 0;
-        for (uint32_t i = lane; i < rn; i += 32 * kLongUnroll) {
-          uint32_t w[kLongUnroll];
+        const uint32_t* row2 = t.vals + rlo2;
+        uint32_t row_hits = 0, row_hits2 = 0;
+        const uint32_t rmax = rn > rn2 ? rn : rn2;
+        for (uint32_t i = lane; i < rmax; i += 32 * kLongUnroll) {
+          uint32_t w[kLongUnroll], w2[kLongUnroll];
 #pragma unroll
-          for (int u = 0; u < kLongUnroll; u++) w[u] = (i + 32 * u < rn) ? __ldg(row + i + 32 * u) : 0u;
+          for (int u = 0; u < kLongUnroll; u++) {
+            w[u] = (i + 32 * u < rn) ? __ldg(row + i + 32 * u) : 0u;
+            w2[u] = (i + 32 * u < rn2) ? __ldg(row2 + i + 32 * u) : 0u;
+          }
 #pragma unroll
           for (int u = 0; u < kLongUnroll; u++) {
             if (i + 32 * u < rn) {
@@ -578,12 +624,21 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
               row_hits += h;
               if (kMode != MODE_COUNT && h) on_hit<kMode, true>(t, r, sk, src_j, w[u]);
             }
+            if (i + 32 * u < rn2) {
+              const uint32_t h = probe<P>(st, w2[u]);
+              row_hits2 += h;
+              if (kMode != MODE_COUNT && h) on_hit<kMode, true>(t, r, sk, src_j2, w2[u]);
+            }
           }
         }
-        cnt += row_hits;
-        if (kMode == MODE_ANNOT) {  // the row's source once per row
+        cnt += row_hits + row_hits2;
+        if (kMode == MODE_ANNOT) {  // each row's source once per row
           const uint32_t rh = warp_sum(row_hits);
-          if (lane == 0) add_src<kMode>(r, sk, src_j, rh);
+          const uint32_t rh2 = warp_sum(row_hits2);
+          if (lane == 0) {
+            add_src<kMode>(r, sk, src_j, rh);
+            if (two) add_src<kMode>(r, sk, src_j2, rh2);
+          }
         }
       }
     }
@@ -640,9 +695,8 @@ __device__ __forceinline__ int stage_set(const TrieView& t, uint32_t hb, uint32_
     if (zbits_words(a.n, len) <= (uint32_t)cap_words) {
       // compressed: 32 words per step, 4 steps of loads in flight
       const uint32_t groups = (a.n + 31) / 32;
-      uint32_t* pres = sm;
-      uint32_t* zr = sm + groups;
-      uint64_t* zw = reinterpret_cast<uint64_t*>(sm + ((2 * groups + 1) & ~1u));
+      uint2* pz = reinterpret_cast<uint2*>(sm);
+      uint64_t* zw = reinterpret_cast<uint64_t*>(sm + 2 * groups);
       const uint64_t* src = t.bs_words + a.off;
       uint32_t run = 0;
       for (uint32_t g0 = 0; g0 < groups; g0 += 4) {
@@ -657,17 +711,13 @@ __device__ __forceinline__ int stage_set(const TrieView& t, uint32_t hb, uint32_
           if (g0 + u < groups) {
             const uint32_t bal = __ballot_sync(kFull, x[u] != 0ull);
             if (x[u]) zw[run + __popc(bal & lanemask_lt())] = x[u];
-            if (lane == 0) {
-              pres[g0 + u] = bal;
-              zr[g0 + u] = run;
-            }
+            if (lane == 0) pz[g0 + u] = make_uint2(bal, run);
             run += __popc(bal);
           }
         }
       }
       __syncwarp();
-      st.pres = pres;
-      st.zrank = zr;
+      st.pz = pz;
       st.words = zw;
       return P_ZBITS;
     }

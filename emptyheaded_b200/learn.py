@@ -99,6 +99,64 @@ def dataset(prof, max_weight=32):
     return np.concatenate(xs), np.concatenate(ys)
 
 
+def on_policy_rows(E, trie, model, query="triangle", config=None, explore=0.5, seed=0, reps=1):
+    """Per-set cycles under a mixed assignment.  The forced-layout profile
+    times every set while all others share its layout; the model's own
+    assignment mixes layouts, and a set's cost depends on its neighbours'
+    (word-level rows need both sides in range bitsets, the annotated pass
+    counts matches in shared memory only for some staged forms).  The trie
+    is laid out by the model, a random `explore` share of the sets it moved
+    goes back to the density rule's layout, the query runs with records, and
+    each staged set's cycles come back with the layout it really had.
+    Returns (features, log1p cycles); the trie is left with the rule's
+    layouts."""
+    trie.relayout()
+    head, off, vals, heur = trie.export()
+    trie.relayout(policy=E.LEARNED, model=model)
+    _, _, _, lay = trie.export()
+    rng = np.random.default_rng(seed)
+    moved = lay != heur
+    back = moved & (rng.random(len(lay)) < explore)
+    lay = np.where(back, heur, lay).astype(np.uint8)
+    trie.relayout(policy=E.EXPLICIT, layouts=lay)
+    n = len(head)
+    acc = np.zeros(n)
+    pairs = np.zeros(n)
+    for _ in range(reps):
+        trie.count(query, record=True, config=config)
+        rec = E.timing_records(trie.ctx)
+        hb = rec[:, 6].view(np.uint32).astype(np.int64)
+        acc += np.bincount(hb, weights=rec[:, 7].astype(np.float64), minlength=n)
+        pairs = np.bincount(hb, weights=rec[:, 1].astype(np.float64), minlength=n)
+    trie.relayout()
+    lens = np.diff(off).astype(np.float64)
+    first = vals[off[:-1].astype(np.int64)].astype(np.float64)
+    last = vals[np.maximum(off[1:].astype(np.int64) - 1, 0)].astype(np.float64)
+    rg = np.where(lens > 0, last - first, 0.0)
+    m = (pairs > 0) & (acc > 0)
+    f = set_features(lens[m], rg[m], pairs[m], lay[m].astype(np.int64))
+    return f, np.log1p(acc[m] / reps).astype(np.float32)[:, None]
+
+
+def refine(E, trie, model, prof, query="triangle", config=None, rounds=1, epochs=40, weight=4, seed=0):
+    """Retrain on the forced-layout profile plus on-policy rows
+    (on_policy_rows, repeated `weight` times) gathered under the current
+    model's assignment, `rounds` times.  Returns (model, info) with info
+    evaluated on the forced profile as before."""
+    x0, y0 = dataset(prof)
+    xs, ys = [x0], [y0]
+    for r in range(rounds):
+        f, y = on_policy_rows(E, trie, model, query=query, config=config, seed=seed + r)
+        xs.append(np.repeat(f, weight, axis=0))
+        ys.append(np.repeat(y, weight, axis=0))
+        model.free()
+        model, _ = train(E, np.concatenate(xs), np.concatenate(ys), ctx=trie.ctx, epochs=epochs, seed=seed + r)
+    info = evaluate(E, model, prof)
+    info["on_policy_rows"] = int(sum(len(x) for x in xs[1:]) // max(1, weight))
+    info["query"] = query
+    return model, info
+
+
 def _fold(params, dims, mu_x, sd_x, mu_y, sd_y):
     """Fold input standardisation into layer 0 and output scaling into the
     last layer, so the device chooser evaluates the model on raw features."""
@@ -146,8 +204,14 @@ def train(E, x, y, ctx=None, epochs=40, batch=2048, lr=0.05, seed=0):
     return model, losses
 
 
-def evaluate(E, model, prof):
-    """Prediction error and regret against the per-set exhaustive search."""
+MIN_GAIN = 0.1  # the device chooser's default margin (eh_layout_config.min_gain = 0)
+
+
+def evaluate(E, model, prof, min_gain=MIN_GAIN):
+    """Prediction error and regret against the per-set exhaustive search.
+    The model's choice is the device chooser's: its predicted-cheapest
+    admissible layout, unless that is predicted to gain less than min_gain
+    over the density rule's layout, which then stays."""
     staged = prof["pairs"] > 0
     n = len(prof["lens"])
     C = np.stack([prof["cycles"][L] for L in LAYOUTS], 1)  # n x 3
@@ -160,9 +224,12 @@ def evaluate(E, model, prof):
     P = np.stack(preds, 1)
     P = np.where(np.isfinite(C), P, np.inf)
     choice = np.argmin(P, 1)
-    chosen = C[np.arange(n), choice]
     heur_col = np.where(prof["heuristic"] == BITSET, 1, 0)  # heuristic uses uint or bitset
-    heur_cost = C[np.arange(n), heur_col]
+    rows = np.arange(n)
+    keep = (choice != heur_col) & ~(P[rows, choice] < P[rows, heur_col] + np.log1p(-min_gain))
+    choice = np.where(keep & np.isfinite(P[rows, heur_col]), heur_col, choice)
+    chosen = C[rows, choice]
+    heur_cost = C[rows, heur_col]
     m = staged & np.isfinite(best) & np.isfinite(chosen) & np.isfinite(heur_cost)
     total_best = best[m].sum()
     finite = np.isfinite(C) & (C > 0)
@@ -175,6 +242,36 @@ def evaluate(E, model, prof):
         "choice_hist": {"uint": int((choice[staged] == 0).sum()), "bitset": int((choice[staged] == 1).sum()),
                         "block": int((choice[staged] == 2).sum())},
     }
+
+
+def judge(E, trie, model, query="triangle", config=None, reps=3):
+    """The density rule as judge: `query` timed on `trie` (engine CUDA
+    events, kernel time, median of `reps` after one warm run) with the
+    rule's layouts and with the model's; the trie keeps the faster
+    assignment.  Layouts change speed only: every count is checked against
+    the first.  Returns {heuristic_ms, learned_ms, kept}."""
+    import statistics
+    want = [None]
+
+    def timed():
+        ks = []
+        for _ in range(reps + 1):
+            c, st = trie.count(query, stats=True, config=config)
+            if want[0] is None:
+                want[0] = c
+            if c != want[0]:
+                raise AssertionError("layouts changed the count: %d != %d" % (c, want[0]))
+            ks.append(st["kernel_ms"])
+        return statistics.median(ks[1:])
+
+    trie.relayout()
+    h = timed()
+    trie.relayout(policy=E.LEARNED, model=model)
+    l = timed()
+    kept = "learned" if l <= h else "heuristic"
+    if kept == "heuristic":
+        trie.relayout()
+    return {"heuristic_ms": h, "learned_ms": l, "kept": kept}
 
 
 def best_layouts(prof):
