@@ -46,6 +46,10 @@ constexpr int kShortUnroll = EH_SHORT_UNROLL;  // flattened (row, element) pairs
 #define EH_WORD_UNROLL 1
 #endif
 constexpr int kWordUnroll = EH_WORD_UNROLL;  // flattened (row, word) pairs per lane per trip
+#ifndef EH_LONG_WORD_UNROLL
+#define EH_LONG_WORD_UNROLL 1
+#endif
+constexpr int kLongWordUnroll = EH_LONG_WORD_UNROLL;  // 16-byte N(a) loads per lane per trip of a long word row
 #ifndef EH_LONG_WORDS
 #define EH_LONG_WORDS 32
 #endif
@@ -484,8 +488,9 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
       uint32_t nw = (word_row && whi >= wlo) ? whi - wlo + 1 : 0u;
       if (word_row) len = 0;  // handled here, not in the element loop
       // long word rows (at least a warp's width of words): one row at a time
-      // across the warp, each lane ANDing words lane, lane + 32, ... with two
-      // independent loads in flight, no owner search
+      // across the warp, each lane ANDing the word pairs 2 lane, 2 lane + 64,
+      // ... read from N(a) with one aligned 16-byte load (the reference's
+      // 128-bit AND), no owner search
       {
         const bool is_long = nw >= (uint32_t)kLongWords;
         uint32_t rows = __ballot_sync(kFull, is_long);
@@ -499,32 +504,50 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
           const uint32_t sj = (kMode != MODE_COUNT) ? __shfl_sync(kFull, src, j) : 0u;
           const uint32_t w_first = b0 >> 6, w_last = b1 >> 6;
           uint32_t row_hits = 0;
-          for (uint32_t w = lo_w + lane; w <= hi_w; w += 64) {
-            const uint32_t w2 = w + 32;
-            const uint64_t a1 = __ldg(t.bs_words + base + w);
-            const uint64_t a2 = w2 <= hi_w ? __ldg(t.bs_words + base + w2) : 0ull;
-            uint64_t m1 = ~0ull, m2 = ~0ull;
-            if (w == w_first) m1 &= ~0ull << (b0 & 63);
-            if (w == w_last) m1 &= ~0ull >> (63 - (b1 & 63));
-            if (w2 == w_first) m2 &= ~0ull << (b0 & 63);
-            if (w2 == w_last) m2 &= ~0ull >> (63 - (b1 & 63));
-            const uint64_t s1 = (P == P_SBITS) ? st.words[w - st.start] : __ldg(st.words + (w - st.start));
-            const uint64_t s2 =
-                w2 <= hi_w ? ((P == P_SBITS) ? st.words[w2 - st.start] : __ldg(st.words + (w2 - st.start))) : 0ull;
-            const uint64_t x1 = a1 & s1 & m1, x2 = a2 & s2 & m2;
-            row_hits += __popcll(x1) + __popcll(x2);
-            if (kMode == MODE_MAT || (kMode == MODE_ANNOT && r.dir == DIR_SYM)) {
-              uint64_t y = x1;
-              while (y) {
-                const uint32_t bit = __ffsll((long long)y) - 1;
-                on_hit<kMode, true>(t, r, sk, sj, (w << 6) | bit);
-                y &= y - 1;
+          // pairs (w, w+1) with base + w even: 16-byte aligned in the word pool
+          // (allocations are at least 16-byte aligned).  A pair may start one
+          // word before lo_w (that word is in the pool: base + lo_w is odd
+          // then, so >= 1) and is masked; a pair is read whole only when w + 1
+          // is still in the row's range, so no read passes N(a)'s last word.
+          const uint32_t wa = lo_w - (uint32_t)((base + lo_w) & 1ull);
+          for (uint32_t w0 = wa + 2 * lane; w0 <= hi_w; w0 += 64 * kLongWordUnroll) {
+            uint64_t x[2 * kLongWordUnroll], y[2 * kLongWordUnroll];
+#pragma unroll
+            for (int u = 0; u < kLongWordUnroll; u++) {
+              const uint32_t w = w0 + 64 * u;
+              if (w + 1 <= hi_w) {
+                const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(t.bs_words + base + w));
+                x[2 * u] = v.x;
+                x[2 * u + 1] = v.y;
+              } else {
+                x[2 * u] = w <= hi_w ? __ldg(t.bs_words + base + w) : 0ull;
+                x[2 * u + 1] = 0ull;
               }
-              y = x2;
-              while (y) {
-                const uint32_t bit = __ffsll((long long)y) - 1;
-                on_hit<kMode, true>(t, r, sk, sj, (w2 << 6) | bit);
-                y &= y - 1;
+#pragma unroll
+              for (int h = 0; h < 2; h++) {
+                const uint32_t wh = w + h;
+                const bool in = wh >= lo_w && wh <= hi_w;
+                y[2 * u + h] = in ? ((P == P_SBITS) ? st.words[wh - st.start] : __ldg(st.words + (wh - st.start))) : 0ull;
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < 2 * kLongWordUnroll; u++) {
+              const uint32_t w = w0 + 64 * (u >> 1) + (u & 1);
+              if (w == w_first) y[u] &= ~0ull << (b0 & 63);
+              if (w == w_last) y[u] &= ~0ull >> (63 - (b1 & 63));
+              x[u] &= y[u];
+              row_hits += __popcll(x[u]);
+            }
+            if (kMode == MODE_MAT || (kMode == MODE_ANNOT && r.dir == DIR_SYM)) {
+#pragma unroll
+              for (int u = 0; u < 2 * kLongWordUnroll; u++) {
+                const uint32_t w = w0 + 64 * (u >> 1) + (u & 1);
+                uint64_t z = x[u];
+                while (z) {
+                  const uint32_t bit = __ffsll((long long)z) - 1;
+                  on_hit<kMode, true>(t, r, sk, sj, (w << 6) | bit);
+                  z &= z - 1;
+                }
               }
             }
           }

@@ -285,6 +285,28 @@ def best_layouts(prof):
     return np.where(staged, pick, prof["heuristic"].astype(np.uint8)).astype(np.uint8)
 
 
+def merge_profiles(profs):
+    """One profile over the sets of several tries (a batch's graphs)."""
+    out = {k: np.concatenate([p[k] for p in profs]) for k in ("lens", "range", "pairs", "heuristic", "words")}
+    out["cycles"] = {L: np.concatenate([p["cycles"][L] for p in profs]) for L in LAYOUTS}
+    return out
+
+
+def train_from_tries(E, tries, passes=2, epochs=60, query="triangle", config=None):
+    """train_from_trie over many tries: each is profiled on its own (the
+    engine's per-item logs of its own runs), the logs are pooled and one
+    model is trained on them.  Returns (model, info, pooled profile)."""
+    prof = merge_profiles([profile(E, t, reps=passes, query=query, config=config) for t in tries])
+    x, y = dataset(prof)
+    model, losses = train(E, x, y, ctx=tries[0].ctx, epochs=epochs)
+    info = evaluate(E, model, prof)
+    info["train_rows"] = int(len(x))
+    info["final_loss"] = float(np.mean(losses[-20:])) if losses else None
+    info["query"] = query
+    info["tries"] = len(tries)
+    return model, info, prof
+
+
 def train_from_trie(E, trie, passes=2, epochs=60, query="triangle", prof=None, config=None):
     """Profile `trie` (or take its profile), train the cost model on the
     logs, evaluate it on the same logs.  Returns (model, info, profile)."""
