@@ -273,12 +273,12 @@ def other_workloads(E, ctx, args, flush, deadline, model22):
             ms_h = run_batch("heuristic")
             # a model trained on the batch's own logs: the even-numbered graphs
             # are profiled, the odd-numbered ones are never seen in training
-            mb, infob, _ = learn.train_from_tries(E, tries[::2], passes=2, epochs=40, config=dict(AT.DEFAULT))
+            mb, infob, _ = learn.train_from_tries(E, tries[::2], passes=1, epochs=30, config=dict(AT.DEFAULT))
             for t in tries:
                 t.relayout(policy=E.LEARNED, model=mb)
             ms_l = run_batch("learned")
             # the density rule as judge, graph by graph: each keeps the faster layouts
-            kept = [learn.judge(E, t, mb, config=dict(AT.DEFAULT))["kept"] for t in tries]
+            kept = [learn.judge(E, t, mb, config=dict(AT.DEFAULT), reps=2)["kept"] for t in tries]
             ms_j = run_batch("judged")
             mb.free()
             rows = int(sum(t.info()["rows"] for t in tries))
@@ -367,6 +367,8 @@ def other_workloads(E, ctx, args, flush, deadline, model22):
                 ql = timed_counts(t, q, cfg, 3, 1, int(g23[q]), flush)[0]
                 rec[q] = {"count": int(g23[q]), "heuristic": _ms(res[q]), "learned": _ms(ql),
                           "learned_speedup": statistics.mean(res[q]) / statistics.mean(ql)}
+            jc = learn.judge(E, t, mc, query="lollipop", config=cfg, reps=2)
+            rec["judged_kept"] = jc["kept"]
             rec["model"] = {k: infoc[k] for k in ("median_abs_pct_error", "regret_learned_pct",
                                                   "regret_heuristic_pct", "sets_staged") if k in infoc}
             t.free()

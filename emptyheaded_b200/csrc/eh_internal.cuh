@@ -12,6 +12,10 @@ struct eh_context {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
   // per-item timing records of the last recorded query (8 floats each)
   std::vector<float> timing_records;
+  // the annotated triangle pass's per-head counters: a cudaMalloc'd buffer of
+  // annot_cap entries kept across queries (see annot_buffer in eh_query.cu)
+  unsigned long long* annot = nullptr;
+  size_t annot_cap = 0;
 };
 
 namespace eh {

@@ -273,6 +273,26 @@ static uint32_t build_plan(eh_context* ctx, const eh_trie* t, const PlanShape& s
   return 1 + 2 * scan_launches(t->n_head) + (h[0] ? 1 : 0) + (h[1] ? 1 : 0);
 }
 
+
+// L2 eviction priority for the word rows' loads of N(a)'s bitset words: the
+// sources of the word rows are the density rule's dense sets (75 MB of words
+// at R-MAT-22, each read ~130 times in a query), so they are kept ahead of the
+// streamed candidate values (createpolicy + ld.global.nc.L2::cache_hint).
+__device__ __forceinline__ uint64_t l2_policy_last() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ ulonglong2 ld2_hint(const uint64_t* a, uint64_t pol) {
+  ulonglong2 v;
+  asm("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;" : "=l"(v.x), "=l"(v.y) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint64_t ld64_hint(const uint64_t* a, uint64_t pol) {
+  uint64_t v;
+  asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(pol));
+  return v;
+}
 // ------------------------------------------------------------------ probes
 // Probe structures for the staged set N(b), one per stored layout.
 // P_ZBITS: a range bitset too large to stage word for word, staged
@@ -458,6 +478,7 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
   constexpr bool kBits = (P == P_SBITS || P == P_GBITS);
   const uint32_t lane = lane_id();
   uint64_t cnt = 0;
+  const uint64_t pol_keep = l2_policy_last();
   for (uint32_t k0 = kb; k0 < ke; k0 += 32) {
     const uint32_t k = k0 + lane;
     uint32_t lo = 0, len = 0, src = 0;
@@ -504,35 +525,43 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
           const uint32_t sj = (kMode != MODE_COUNT) ? __shfl_sync(kFull, src, j) : 0u;
           const uint32_t w_first = b0 >> 6, w_last = b1 >> 6;
           uint32_t row_hits = 0;
-          // pairs (w, w+1) with base + w even: 16-byte aligned in the word pool
-          // (allocations are at least 16-byte aligned).  A pair may start one
-          // word before lo_w (that word is in the pool: base + lo_w is odd
-          // then, so >= 1) and is masked; a pair is read whole only when w + 1
-          // is still in the row's range, so no read passes N(a)'s last word.
-          const uint32_t wa = lo_w - (uint32_t)((base + lo_w) & 1ull);
-          for (uint32_t w0 = wa + 2 * lane; w0 <= hi_w; w0 += 64 * kLongWordUnroll) {
+          // The row's words lo_w..hi_w are read in pairs from an even pool
+          // index, 16-byte aligned (allocations are at least 16-byte
+          // aligned): pair q holds the row's words q - par and q + 1 - par,
+          // where par = 1 when the row starts at an odd pool index (its first
+          // pair then begins with the word before lo_w: in the pool, since
+          // that index is >= 1, and masked).  Offsets stay non-negative; a
+          // word index is formed only for words inside the row.  A pair is
+          // read whole only when both its words are in the row's range or the
+          // first one is the word before it, so no read passes N(a)'s last word.
+          const uint32_t par = (uint32_t)((base + lo_w) & 1ull);
+          const uint32_t end = hi_w - lo_w + 1 + par;         // pair offsets run below end
+          const uint64_t g0 = base + lo_w - par;              // even pool index of offset 0
+          const uint32_t wa = lo_w - par;                     // word of offset 0 (mod 2^32)
+          const uint32_t sa = wa - st.start;                  // its staged index (mod 2^32)
+          for (uint32_t q0 = 2 * lane; q0 < end; q0 += 64 * kLongWordUnroll) {
             uint64_t x[2 * kLongWordUnroll], y[2 * kLongWordUnroll];
 #pragma unroll
             for (int u = 0; u < kLongWordUnroll; u++) {
-              const uint32_t w = w0 + 64 * u;
-              if (w + 1 <= hi_w) {
-                const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(t.bs_words + base + w));
+              const uint32_t q = q0 + 64 * u;
+              if (q + 2 <= end) {
+                const ulonglong2 v = ld2_hint(t.bs_words + g0 + q, pol_keep);
                 x[2 * u] = v.x;
                 x[2 * u + 1] = v.y;
               } else {
-                x[2 * u] = w <= hi_w ? __ldg(t.bs_words + base + w) : 0ull;
+                x[2 * u] = q < end ? ld64_hint(t.bs_words + g0 + q, pol_keep) : 0ull;
                 x[2 * u + 1] = 0ull;
               }
 #pragma unroll
               for (int h = 0; h < 2; h++) {
-                const uint32_t wh = w + h;
-                const bool in = wh >= lo_w && wh <= hi_w;
-                y[2 * u + h] = in ? ((P == P_SBITS) ? st.words[wh - st.start] : __ldg(st.words + (wh - st.start))) : 0ull;
+                const uint32_t qh = q + h;
+                const bool in = qh >= par && qh < end;  // a word of the row
+                y[2 * u + h] = in ? ((P == P_SBITS) ? st.words[sa + qh] : __ldg(st.words + (sa + qh))) : 0ull;
               }
             }
 #pragma unroll
             for (int u = 0; u < 2 * kLongWordUnroll; u++) {
-              const uint32_t w = w0 + 64 * (u >> 1) + (u & 1);
+              const uint32_t w = wa + (q0 + 64 * (u >> 1) + (u & 1));  // meaningful where y is non-zero
               if (w == w_first) y[u] &= ~0ull << (b0 & 63);
               if (w == w_last) y[u] &= ~0ull >> (63 - (b1 & 63));
               x[u] &= y[u];
@@ -541,8 +570,8 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
             if (kMode == MODE_MAT || (kMode == MODE_ANNOT && r.dir == DIR_SYM)) {
 #pragma unroll
               for (int u = 0; u < 2 * kLongWordUnroll; u++) {
-                const uint32_t w = w0 + 64 * (u >> 1) + (u & 1);
-                uint64_t z = x[u];
+                uint64_t z = x[u];  // non-zero only for words inside the row
+                const uint32_t w = wa + (q0 + 64 * (u >> 1) + (u & 1));
                 while (z) {
                   const uint32_t bit = __ffsll((long long)z) - 1;
                   on_hit<kMode, true>(t, r, sk, sj, (w << 6) | bit);
@@ -583,7 +612,7 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
             if (w == (b0 >> 6)) m &= ~0ull << (b0 & 63);
             if (w == (b1 >> 6)) m &= ~0ull >> (63 - (b1 & 63));
             const uint64_t bw = (P == P_SBITS) ? st.words[w - st.start] : __ldg(st.words + (w - st.start));
-            x[u] = __ldg(t.bs_words + base + w) & bw & m;
+            x[u] = ld64_hint(t.bs_words + base + w, pol_keep) & bw & m;
             wv[u] = w;
           }
         }
@@ -1378,6 +1407,10 @@ static void prepare(eh_context* ctx, const eh_trie* const* tries, uint32_t n, in
   for (uint32_t g = 0; g < n; g++) {
     hv[g] = tries[g]->view();
     hr[g] = rev_view(tries[g]);
+    // the intersection kernels read the values and the bitset words with
+    // 16-byte loads at 16-byte aligned indices
+    if ((reinterpret_cast<uintptr_t>(hv[g].vals) | reinterpret_cast<uintptr_t>(hv[g].bs_words)) & 15u)
+      throw Error{EH_ERR_UNSUPPORTED, "trie arrays are not 16-byte aligned"};
   }
   P.dv.alloc(n, s);
   P.dr.alloc(n, s);
@@ -1573,6 +1606,29 @@ void query_weighted_root(eh_context* ctx, const eh_trie* t, int query, const uin
   *result = h;
 }
 
+// The annotated pass's per-head counters take one global atomic per hit
+// (2.8 G on Chung-Lu 2^23).  Measured on B200 (Chung-Lu 2^23 lollipop): with
+// the counters in the stream-ordered pool the pass ran at 243 or 184 ms
+// depending on where the pool placed them (holding a 128 MB allocation before
+// the query flipped it); in an allocation of their own from cudaMalloc it ran
+// at 184 ms whatever the pool held.  The context keeps one such buffer, grown
+// (with the stream drained first) when a larger trie needs it.
+static unsigned long long* annot_buffer(eh_context* ctx, size_t n) {
+  if (n > ctx->annot_cap) {
+    EH_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->annot) EH_CUDA(cudaFree(ctx->annot));
+    ctx->annot = nullptr;
+    ctx->annot_cap = 0;
+    if (cudaMalloc((void**)&ctx->annot, n * sizeof(unsigned long long)) != cudaSuccess) {
+      cudaGetLastError();
+      ctx->annot = nullptr;
+      throw Error{EH_ERR_OOM, "device allocation of " + std::to_string(n * 8) + " bytes failed"};
+    }
+    ctx->annot_cap = n;
+  }
+  return ctx->annot;
+}
+
 void query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t n, int query,
                          const eh_exec_config* cfg, uint64_t* results, eh_query_stats* stats) {
   cudaStream_t s = ctx->stream;
@@ -1615,11 +1671,12 @@ void query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t 
       rec.alloc(8 * (t->n_head + t->rev_pairs / ep.chunk + 16), s);
       recp = rec.p;
     }
-    DevBuf<unsigned long long> T(t->n_head ? t->n_head : 1, s), dummy(1, s);
-    EH_CUDA(cudaMemsetAsync(T.p, 0, (t->n_head ? t->n_head : 1) * 8, s));
+    unsigned long long* T = annot_buffer(ctx, t->n_head ? t->n_head : 1);
+    DevBuf<unsigned long long> dummy(1, s);
+    EH_CUDA(cudaMemsetAsync(T, 0, (t->n_head ? t->n_head : 1) * 8, s));
     EH_CUDA(cudaMemsetAsync(dummy.p, 0, 8, s));
-    L = run_plans(ctx, tries, 1, EH_QUERY_TRIANGLE, ep, true, dummy.p, T.p, recp, &items, &pairs);
-    L.launches += root_bag(ctx, t, query, T.p, nullptr, total.p);
+    L = run_plans(ctx, tries, 1, EH_QUERY_TRIANGLE, ep, true, dummy.p, T, recp, &items, &pairs);
+    L.launches += root_bag(ctx, t, query, T, nullptr, total.p);
   }
   std::vector<unsigned long long> h(n);
   EH_CUDA(cudaMemcpyAsync(h.data(), total.p, n * 8, cudaMemcpyDeviceToHost, s));

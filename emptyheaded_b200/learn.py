@@ -79,11 +79,13 @@ def profile(E, trie, reps=2, query="triangle", config=None):
     return dict(lens=lens, range=rng, pairs=pairs, cycles=cycles, heuristic=heur.astype(np.int64), words=words)
 
 
-def dataset(prof, max_weight=32):
+def dataset(prof, max_weight=32, max_rows=2_000_000, seed=0):
     """Training rows (features, log1p cycles), one per staged set and
     admissible layout.  A set's row is repeated in proportion to its cost
     (at most max_weight times): the sets that hold the time are the ones the
-    choice has to get right, and most sets are cheap."""
+    choice has to get right, and most sets are cheap.  Above max_rows rows
+    a seeded uniform sample of max_rows is kept (training time grows with
+    the rows; a power-law graph has millions of staged sets)."""
     xs, ys = [], []
     staged = prof["pairs"] > 0
     for L in LAYOUTS:
@@ -96,7 +98,11 @@ def dataset(prof, max_weight=32):
         y = np.log1p(c[m]).astype(np.float32)[:, None]
         xs.append(np.repeat(f, reps, axis=0))
         ys.append(np.repeat(y, reps, axis=0))
-    return np.concatenate(xs), np.concatenate(ys)
+    x, y = np.concatenate(xs), np.concatenate(ys)
+    if max_rows and len(x) > max_rows:
+        keep = np.sort(np.random.default_rng(seed).choice(len(x), max_rows, replace=False))
+        x, y = x[keep], y[keep]
+    return x, y
 
 
 def on_policy_rows(E, trie, model, query="triangle", config=None, explore=0.5, seed=0, reps=1):
