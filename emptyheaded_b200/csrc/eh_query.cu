@@ -50,6 +50,14 @@ constexpr int kWordUnroll = EH_WORD_UNROLL;  // flattened (row, word) pairs per 
 #define EH_LONG_WORD_UNROLL 1
 #endif
 constexpr int kLongWordUnroll = EH_LONG_WORD_UNROLL;  // 16-byte N(a) loads per lane per trip of a long word row
+#ifndef EH_WORD_ROW_NUM
+#define EH_WORD_ROW_NUM 1
+#endif
+#ifndef EH_WORD_ROW_DEN
+#define EH_WORD_ROW_DEN 1
+#endif
+// a row runs word by word when words * num < candidates * den
+constexpr uint32_t kWordRowNum = EH_WORD_ROW_NUM, kWordRowDen = EH_WORD_ROW_DEN;
 #ifndef EH_LONG_WORDS
 #define EH_LONG_WORDS 32
 #endif
@@ -465,8 +473,9 @@ __device__ __forceinline__ void add_src(const RevView& r, const Sink& sk, uint32
 
 // Rows whose source set N(a) is also a range bitset, against a bitset N(b),
 // are intersected word by word (64-bit AND + popcount over the overlap of
-// the candidate value range [v0, v1] with both word ranges) whenever that
-// takes fewer words than the row has candidate elements; the reference's
+// the candidate value range [v0, v1] with both word ranges) whenever the
+// words, weighted by kWordRowNum / kWordRowDen (a word against a candidate
+// probe), are fewer than the row's candidate elements; the reference's
 // bitset ∩ bitset path (ops/intersection/bitset.hpp:526-567, 619-661).
 // Word rows run warp-cooperatively one row at a time (coalesced 8-byte
 // loads of N(a)'s words); the other rows are flattened (row, element)
@@ -499,7 +508,7 @@ __device__ __forceinline__ uint64_t stream_rows(const Staged& st, const TrieView
         const uint32_t lo_w = max(max(v0 >> 6, aa.start), st.start);
         const uint32_t hi_w = min(min(v1 >> 6, aa.start + aa.n - 1), st.start + st.n - 1);
         const uint32_t words = hi_w >= lo_w ? hi_w - lo_w + 1 : 0;
-        if (words < len) {
+        if (words * kWordRowNum < len * kWordRowDen) {
           word_row = true;
           wlo = lo_w;
           whi = hi_w;
