@@ -136,47 +136,29 @@ __device__ __forceinline__ uint64_t first_row_at(const uint64_t* __restrict__ wp
   return lo;
 }
 
-// A lane cuts the items of its own head entry one after the other; an
-// entry with more than kFillSerial items (a hub b) is cut by the whole
-// warp, each lane bounding its items with two independent searches, so one
-// thread never holds the planner up for hundreds of searches.  The bounds
-// are the same either way: the work prefix is non-decreasing, so the first
-// row at target i+1 searched from k0 is the one searched from item i's end.
-constexpr uint32_t kFillSerial = 8;
+// One thread per item: item q belongs to the last head entry b with
+// ipos[b] <= q (ipos is the exclusive scan of the items per entry, so entries
+// without items share the next entry's offset and are never found), is item
+// i = q - ipos[b] of b, and covers the rows from the first one at target i to
+// the first one at target i + 1 -- two independent searches over b's rows.
+// The work prefix is non-decreasing, so these are the bounds a serial cut of
+// b's items one after the other finds, at any number of items per entry.
 __global__ void plan_fill_kernel(RevView r, uint32_t nh, const uint32_t* __restrict__ nitems,
                                  const uint32_t* __restrict__ ipos, uint32_t total, uint32_t g,
                                  Item* __restrict__ items) {
-  const uint32_t lane = lane_id();
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint64_t base = (uint64_t)warp * 32; base < nh; base += (uint64_t)nwarps * 32) {
-    const uint32_t b = (uint32_t)base + lane;
-    const uint32_t n = b < nh ? nitems[b] : 0u;
-    if (n && n <= kFillSerial) {
-      const uint64_t k0 = r.rev_off[b], k1 = r.rev_off[b + 1];
-      const uint64_t w0 = r.rev_wpre[k0], W = r.rev_wpre[k1] - w0;
-      uint64_t kb = k0;
-      for (uint32_t i = 0; i < n; i++) {
-        const uint64_t ke = i + 1 < n ? first_row_at(r.rev_wpre, kb, k1, w0 + (W * (i + 1)) / n) : k1;
-        items[total - 1 - (ipos[b] + i)] = Item{b, (uint32_t)kb, (uint32_t)ke, g};
-        kb = ke;
-      }
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = nh;  // first entry with ipos > q
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (ipos[mid] <= q) lo = mid + 1; else hi = mid;
     }
-    uint32_t hubs = __ballot_sync(kFull, n > kFillSerial);
-    while (hubs) {
-      const int j = __ffs(hubs) - 1;
-      hubs &= hubs - 1;
-      const uint32_t bj = (uint32_t)base + j;
-      const uint32_t nj = __shfl_sync(kFull, n, j);
-      const uint64_t k0 = r.rev_off[bj], k1 = r.rev_off[bj + 1];
-      const uint64_t w0 = r.rev_wpre[k0], W = r.rev_wpre[k1] - w0;
-      const uint32_t p0 = ipos[bj];
-      for (uint32_t i = lane; i < nj; i += 32) {
-        const uint64_t kb = i ? first_row_at(r.rev_wpre, k0, k1, w0 + (W * i) / nj) : k0;
-        const uint64_t ke = i + 1 < nj ? first_row_at(r.rev_wpre, kb, k1, w0 + (W * (i + 1)) / nj) : k1;
-        items[total - 1 - (p0 + i)] = Item{bj, (uint32_t)kb, (uint32_t)ke, g};
-      }
-    }
+    const uint32_t b = lo - 1;  // q < total = ipos[nh-1] + nitems[nh-1], so lo >= 1
+    const uint32_t i = q - ipos[b], n = nitems[b];
+    const uint64_t k0 = r.rev_off[b], k1 = r.rev_off[b + 1];
+    const uint64_t w0 = r.rev_wpre[k0], W = r.rev_wpre[k1] - w0;
+    const uint64_t kb = i ? first_row_at(r.rev_wpre, k0, k1, w0 + (W * i) / n) : k0;
+    const uint64_t ke = i + 1 < n ? first_row_at(r.rev_wpre, kb, k1, w0 + (W * (i + 1)) / n) : k1;
+    items[total - 1 - q] = Item{b, (uint32_t)kb, (uint32_t)ke, g};
   }
 }
 
@@ -262,6 +244,7 @@ static uint32_t build_plan(eh_context* ctx, const eh_trie* t, const PlanShape& s
   ps.unit = t->pred_per_probe * shape.chunk;
   DevBuf<uint32_t> nw(t->n_head, s), nb(t->n_head, s), pw(t->n_head, s), pb(t->n_head, s), tot(2, s);
   const int grid = num_sms() * 4;
+  TracePhase ph_split("plan.split+scan", s);
   plan_split_kernel<<<grid, 256, 0, s>>>(t->view(), r, ps, nw.p, nb.p);
   EH_CHECK_LAUNCH();
   exclusive_scan<uint32_t>(nw.p, pw.p, t->n_head, tot.p, s);
@@ -269,6 +252,8 @@ static uint32_t build_plan(eh_context* ctx, const eh_trie* t, const PlanShape& s
   uint32_t h[2] = {0, 0};
   EH_CUDA(cudaMemcpyAsync(h, tot.p, 8, cudaMemcpyDeviceToHost, s));
   EH_CUDA(cudaStreamSynchronize(s));
+  ph_split.end();
+  TracePhase ph_fill("plan.fill", s);
   plan.nb = h[1];
   plan.n = h[0] + h[1];
   plan.items.alloc(plan.n ? plan.n : 1, s);
@@ -1538,14 +1523,20 @@ static Launch run_plans(eh_context* ctx, const eh_trie* const* tries, uint32_t n
   cudaStream_t s = ctx->stream;
   Launch L;
   Prepared P;
-  prepare(ctx, tries, n, query, ep, annot, P, true);
+  {
+    TracePhase ph("query.prepare", s);
+    prepare(ctx, tries, n, query, ep, annot, P, true);
+  }
   P.sel = sel;
   L.launches = P.plan_launches;
   *n_items_out = P.n_items;
   *pairs_out = P.pairs;
   if (!P.n_items) return L;
   EH_CUDA(cudaEventRecord(ctx->ev1, s));
-  launch(ctx, P, d_total, d_annot, d_records);
+  {
+    TracePhase ph("query.kernel", s);
+    launch(ctx, P, d_total, d_annot, d_records);
+  }
   EH_CUDA(cudaEventRecord(ctx->ev2, s));
   L.launches += 1;
   EH_CUDA(cudaEventSynchronize(ctx->ev2));
@@ -1702,6 +1693,7 @@ void query_count_batched(eh_context* ctx, const eh_trie* const* tries, uint32_t 
     for (uint32_t g = 0; g < n; g++) mx = std::max(mx, tries[g]->info.max_set);
     size_clique_staging(ep, mx);
   }
+  TracePhase ph_all("query.total", s);
   EH_CUDA(cudaEventRecord(ctx->ev0, s));
   DevBuf<unsigned long long> total(n, s);
   EH_CUDA(cudaMemsetAsync(total.p, 0, n * 8, s));
