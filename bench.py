@@ -231,7 +231,7 @@ def _ms(x):
 
 # --------------------------------------------------- the other workloads
 def other_workloads(E, ctx, args, flush, deadline, model22):
-    """North-star configs beside the headline: the 256-graph batch, the
+    """The other benchmark workloads beside the headline: the 256-graph batch, the
     R-MAT-20 4-clique, Chung-Lu 2^23 lollipop and barbell; each with the
     density-rule and learned layouts on the device (identical counts) and the
     reference engine on this host's cores (in the same run) on a stated
@@ -568,7 +568,7 @@ def ours_arm(args):
     d.free()
     trie.free()
 
-    # ---- the north-star configs beside the headline (single GPU)
+    # ---- the other benchmark workloads beside the headline (single GPU)
     workloads = None
     if world == 1 and not args.no_extra and model is not None:
         workloads = other_workloads(E, ctx, args, flush, t_start + args.budget_s, model)
@@ -657,7 +657,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline legs")
-    ap.add_argument("--no-extra", action="store_true", help="headline only: skip the other north-star configs")
+    ap.add_argument("--no-extra", action="store_true", help="headline only: skip the batch, 4-clique and lollipop/barbell workloads")
     ap.add_argument("--budget-s", type=float, default=420.0,
                     help="wall-clock budget after which the remaining other configs are skipped")
     ap.add_argument("--case", action="store_true", help="profiler case instead of the bench line")
