@@ -57,13 +57,17 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <functional>
 #include <iostream>
 #include <map>
 #include <memory>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <tuple>
+#include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "../eh_b200.h"
@@ -109,6 +113,87 @@ static inline double stop_clock(std::string in, std::chrono::time_point<std::chr
   return t;
 }
 }  // namespace timer
+
+// -------------------------------------------------------------- Encoding
+// A relation's dictionary (storage_engine/include/Encoding.hpp:21-37): key i
+// stands for key_to_value[i]; value_to_key maps back.  build() gives keys in
+// the order the values come (a std::set: ascending, Encoding.cpp:21-37); a
+// value given twice keeps its first key and still takes a key number, as
+// there.  encode_column maps a column through value_to_key and throws on a
+// value the dictionary lacks (the reference's .at).  to_binary / from_binary
+// write and read <path>encoding.bin: the uint32 count, then every value in key
+// order as its bytes (strings: a size_t length, then the characters), the
+// reference's file (Encoding.cpp:52-130), so dictionaries pass between the
+// engines.  Host code: the device dictionary of eh_encoding_* builds the same
+// keys for uint32/uint64 columns (ascending values).
+template <class T>
+struct Encoding {
+  uint32_t num_distinct = 0;
+  std::vector<T> key_to_value;
+  std::unordered_map<T, uint32_t> value_to_key;
+
+  void build(std::set<T>* values) {
+    for (const T& v : *values) add(v);
+  }
+  void build(std::vector<T>* values) {
+    for (const T& v : *values) add(v);
+  }
+  std::vector<uint32_t>* encode_column(T* column, const size_t length) {
+    std::unique_ptr<std::vector<uint32_t>> out(new std::vector<uint32_t>(length));
+    for (size_t i = 0; i < length; i++) (*out)[i] = value_to_key.at(column[i]);
+    return out.release();
+  }
+  void to_binary(const std::string path) {
+    std::ofstream f(path + "encoding.bin", std::ios::binary | std::ios::out);
+    if (!f) throw std::runtime_error("cannot write " + path + "encoding.bin");
+    f.write(reinterpret_cast<const char*>(&num_distinct), sizeof(num_distinct));
+    for (uint32_t k = 0; k < num_distinct; k++) write_value(f, key_to_value.at(k));
+    if (!f) throw std::runtime_error("write of " + path + "encoding.bin failed");
+  }
+  static Encoding<T>* from_binary(const std::string path) {
+    std::ifstream f(path + "encoding.bin", std::ios::binary | std::ios::in);
+    if (!f) throw std::runtime_error("cannot read " + path + "encoding.bin");
+    std::unique_ptr<Encoding<T>> e(new Encoding<T>());
+    uint32_t n = 0;
+    f.read(reinterpret_cast<char*>(&n), sizeof(n));
+    if (!f) throw std::runtime_error(path + "encoding.bin is truncated");
+    e->key_to_value.reserve(n);
+    e->value_to_key.reserve(n);
+    for (uint32_t k = 0; k < n; k++) {
+      T v;
+      read_value(f, v);
+      if (!f) throw std::runtime_error(path + "encoding.bin is truncated");
+      e->add(v);
+    }
+    return e.release();
+  }
+
+ private:
+  void add(const T& v) {
+    value_to_key.insert(std::make_pair(v, num_distinct++));
+    key_to_value.push_back(v);
+  }
+  static void write_value(std::ofstream& f, const T& v) {
+    if constexpr (std::is_same<T, std::string>::value) {
+      const size_t len = v.size();
+      f.write(reinterpret_cast<const char*>(&len), sizeof(len));
+      f.write(v.data(), (std::streamsize)len);
+    } else {
+      f.write(reinterpret_cast<const char*>(&v), sizeof(T));
+    }
+  }
+  static void read_value(std::ifstream& f, T& v) {
+    if constexpr (std::is_same<T, std::string>::value) {
+      size_t len = 0;
+      f.read(reinterpret_cast<char*>(&len), sizeof(len));
+      if (!f) return;
+      v.assign(len, '\0');
+      f.read(&v[0], (std::streamsize)len);
+    } else {
+      f.read(reinterpret_cast<char*>(&v), sizeof(T));
+    }
+  }
+};
 
 // ------------------------------------------------------------------ engine
 namespace ehd {

@@ -105,3 +105,65 @@ def test_c_translation_unit_against_the_abi(tmp_path):
     assert r.returncode == 0
     status = int(r.stdout.split()[0])
     assert status in (0, 7)  # EH_OK on a GPU box, EH_ERR_NO_DEVICE here
+
+
+def test_encoding_files_match_the_reference_format(tmp_path):
+    """Encoding<T> writes the reference's encoding.bin (Encoding.cpp:52-130):
+    the uint32 count, then the values in key order (a std::set gives
+    ascending keys), strings as a size_t length and the characters; it reads
+    them back, encodes columns through value_to_key, and keeps the
+    reference's build() semantics for a vector with a repeated value."""
+    import json
+    import struct
+    import subprocess
+
+    from conftest import CPP, ROOT
+    exe = str(tmp_path / "dropin_encoding")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"),
+                    "-I" + os.path.join(ROOT, "include", "eh"), os.path.join(CPP, "dropin_encoding.cpp"),
+                    os.path.join(CPP, "fake_eh_abi.cpp"), "-o", exe], check=True, capture_output=True, text=True)
+    r = subprocess.run([exe, str(tmp_path)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    out = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+
+    def file_bytes(sub):
+        return (tmp_path / sub / "encoding.bin").read_bytes()
+
+    assert file_bytes("u32") == struct.pack("<I4I", 4, 3, 5, 7, 900)
+    assert file_bytes("long") == struct.pack("<I3q", 3, -2, 0, 1 << 40)
+    want = struct.pack("<I", 3)
+    for s in ("", "alpha", "b"):
+        want += struct.pack("<Q", len(s)) + s.encode()
+    assert file_bytes("str") == want
+    assert out["u32"] == {"num_distinct": 4, "key_to_value": [3, 5, 7, 900], "encoded": [2, 0, 3, 0],
+                          "lookups": [2, 0, 3, 0]}
+    assert out["long"]["key_to_value"] == [-2, 0, 1 << 40] and out["long"]["encoded"] == [1, 2, 0]
+    assert out["str"]["key_to_value"] == ["", "alpha", "b"] and out["str"]["encoded"] == [1, 0, 2]
+    assert out["vector_num_distinct"] == 4 and out["vector_key_of_40"] == 0
+    assert out["vector_key_to_value"] == [40, 10, 40, 20]
+    assert out["unknown_throws"] is True
+
+
+def test_encoding_files_equal_the_reference_engines(tmp_path):
+    """The same dictionaries written by the reference's own Encoding<T>
+    (oracle/ref_encoding.cpp, compiled from the reference's sources by
+    `make -C oracle ref_encoding`) are byte-identical to the layer's."""
+    import subprocess
+
+    from conftest import CPP, ROOT
+    from oracle import oracle as O
+    if not os.path.isdir(os.path.join(O.reference_dir(), "storage_engine", "src")):
+        pytest.skip("needs the reference checkout ($EH_REFERENCE)")
+    mk = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref_encoding"], capture_output=True, text=True)
+    assert mk.returncode == 0, mk.stderr[-2000:]
+    ref_dir, our_dir = tmp_path / "ref", tmp_path / "ours"
+    ref_dir.mkdir()
+    our_dir.mkdir()
+    subprocess.run([os.path.join(ROOT, "oracle", "_ref", "eh_ref_encoding"), str(ref_dir)], check=True, timeout=60)
+    exe = str(tmp_path / "dropin_encoding")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"),
+                    "-I" + os.path.join(ROOT, "include", "eh"), os.path.join(CPP, "dropin_encoding.cpp"),
+                    os.path.join(CPP, "fake_eh_abi.cpp"), "-o", exe], check=True, capture_output=True, text=True)
+    subprocess.run([exe, str(our_dir)], check=True, capture_output=True, timeout=60)
+    for sub in ("u32", "long", "str"):
+        assert (our_dir / sub / "encoding.bin").read_bytes() == (ref_dir / sub / "encoding.bin").read_bytes(), sub
