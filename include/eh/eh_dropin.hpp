@@ -360,6 +360,7 @@ class Set {
   size_t number_of_bytes = 0;
   type::layout type = type::NOT_VALID;
   const uint32_t* elems = nullptr;  // sorted elements (host)
+  std::shared_ptr<std::vector<uint32_t>> store;  // owned elements of a set ops:: produced
 
   Set() {}
   void view(const uint32_t* p, size_t n) {
@@ -394,6 +395,67 @@ class Set {
     return cardinality;
   }
 };
+
+// ------------------------------------------------------------------- ops
+// ops::set_intersect (trie/set/ops/intersection/set.hpp:9-167), all four
+// forms with the reference's overload shapes (the plain forms are not
+// templates, so a call with three set pointers picks the materialising one),
+// over the layer's host set views: A ∩ B is computed on the device
+// (eh_set_intersect_batch, whatever the sets' layouts); the materialising
+// forms give C its own storage of the result (sorted, its layout by the
+// density rule, as hybrid::build picks it), and the callback forms call
+// f(x, index of x in A, index of x in B) for every element in order, as the
+// reference's do.  For host code over sets already read (a Trie's foreach,
+// the blocks an iterator returns); inside a bag's lambda the builders'
+// build_aggregated_set is the entry the generated code uses.
+namespace ops {
+namespace detail {
+template <class T>
+inline std::vector<uint32_t> intersect(const Set<T>* A, const Set<T>* B) {
+  std::vector<uint32_t> out;
+  ehd::intersect(A->elems, A->cardinality, B->elems, B->cardinality, out);
+  return out;
+}
+template <class T, typename F>
+inline void each(const Set<T>* A, const Set<T>* B, const std::vector<uint32_t>& r, F& f) {
+  uint32_t ia = 0, ib = 0;
+  for (const uint32_t x : r) {  // both sets are sorted and x is in both
+    while (A->elems[ia] < x) ia++;
+    while (B->elems[ib] < x) ib++;
+    f(x, ia, ib);
+  }
+}
+template <class T>
+inline Set<T>* own(Set<T>* C, std::vector<uint32_t>&& r) {
+  C->store = std::make_shared<std::vector<uint32_t>>(std::move(r));
+  C->view(C->store->data(), C->store->size());
+  if (!C->cardinality) {
+    C->type = type::UINTEGER;
+    C->number_of_bytes = 0;
+  }
+  return C;
+}
+}  // namespace detail
+
+template <typename F>
+inline Set<hybrid>* set_intersect(Set<hybrid>* C, const Set<hybrid>* A, const Set<hybrid>* B, F f) {
+  std::vector<uint32_t> r = detail::intersect(A, B);
+  detail::each(A, B, r, f);
+  return detail::own(C, std::move(r));
+}
+inline Set<hybrid>* set_intersect(Set<hybrid>* C, const Set<hybrid>* A, const Set<hybrid>* B) {
+  return detail::own(C, detail::intersect(A, B));
+}
+template <typename F>
+inline size_t set_intersect(const Set<hybrid>* A, const Set<hybrid>* B, F f) {
+  const std::vector<uint32_t> r = detail::intersect(A, B);
+  detail::each(A, B, r, f);
+  return r.size();
+}
+inline size_t set_intersect(const Set<hybrid>* A, const Set<hybrid>* B) {
+  return detail::intersect(A, B).size();
+}
+}  // namespace ops
 
 // --------------------------------------------------------------- TrieBlock
 // A set of a trie level as the generated code sees it, tagged with the

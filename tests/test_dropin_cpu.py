@@ -167,3 +167,33 @@ def test_encoding_files_equal_the_reference_engines(tmp_path):
     subprocess.run([exe, str(our_dir)], check=True, capture_output=True, timeout=60)
     for sub in ("u32", "long", "str"):
         assert (our_dir / sub / "encoding.bin").read_bytes() == (ref_dir / sub / "encoding.bin").read_bytes(), sub
+
+
+def test_set_intersect_forms(tmp_path):
+    """ops::set_intersect in its four forms (trie/set/ops/intersection/
+    set.hpp:9-167) over the layer's sets: the materialising forms give C the
+    sorted intersection with its density-rule layout, the callback forms call
+    f(x, index in A, index in B) per element in order, and an empty side
+    gives an empty result."""
+    import json
+    import subprocess
+
+    from conftest import CPP, ROOT
+    exe = str(tmp_path / "dropin_setops")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"),
+                    "-I" + os.path.join(ROOT, "include", "eh"), os.path.join(CPP, "dropin_setops.cpp"),
+                    os.path.join(CPP, "fake_eh_abi.cpp"), "-o", exe], check=True, capture_output=True, text=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    out = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+    a = [1, 5, 9, 64, 65, 300, 1000, 5000, 70000]
+    b = list(range(256)) + list(range(990, 1010)) + [70000]
+    want = sorted(set(a) & set(b))
+    assert out["c1"] == want and out["c2"] == want
+    assert out["triples"] == [[x, a.index(x), b.index(x)] for x in want]
+    assert out["count_f"] == out["calls"] == out["count"] == len(want)
+    assert out["count_empty"] == 0 and out["c3_cardinality"] == 0
+    assert out["c1_range"] == want[-1]
+    # the density rule (common::is_sparse): 6 elements over 70,000 values are a
+    # uint list, B (277 elements over 70,001 values) too
+    assert out["c1_type"] == 1 and out["b_type"] == 1
