@@ -80,7 +80,10 @@ eh_status eh_context_sync(eh_context* ctx);
 eh_status eh_context_stream(eh_context* ctx, void** stream);
 /* Engine memory pool of the context's device (no counterpart in the
  * reference, which allocates from the host heap per call): bytes the pool
- * holds, bytes in use, and the peak in use since the last reserve. */
+ * holds, bytes in use, and the peak in use since the last reserve.  Not
+ * counted: the lollipop / barbell COUNT's per-head counters (8 bytes per head
+ * entry of the largest trie queried so), a separate device allocation the
+ * context keeps until it is destroyed. */
 eh_status eh_context_memory(eh_context* ctx, uint64_t* reserved, uint64_t* used, uint64_t* peak);
 /* Returns the pool's unused memory to the driver and reserves `bytes` as one
  * block that later allocations are carved from, so that calls whose peak fits
